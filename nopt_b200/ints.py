@@ -1,0 +1,166 @@
+"""ctypes front end of the host integral engine (libgto_ints.so, include/gto_ints.h).
+
+These are the inputs of the RI-JK Fock build that the reference gets from libint2:
+S, T, V (src/molecule.cpp:3757-3800), the metric (P|Q) (RI_V_calc,
+src/libint_link.cpp:2049-2107) and the three-centre (mu nu|P) (calc_2el_AO_INTS_RI,
+src/libint_link.cpp:2261-2350).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import basis as _basis
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+LAYOUT_NOPT_FULL = 0
+LAYOUT_PACKED = 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "libgto_ints.so")
+        if not os.path.exists(path):
+            raise RuntimeError("libgto_ints.so is not built; run __graft_entry__.build()")
+        L = ctypes.CDLL(path)
+        L.gto_basis_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _dp]
+        L.gto_basis_destroy.argtypes = [ctypes.c_void_p]
+        L.gto_basis_destroy.restype = None
+        L.gto_basis_nbf.argtypes = [ctypes.c_void_p]
+        L.gto_basis_max_l.argtypes = [ctypes.c_void_p]
+        L.gto_basis_norm_coefs.argtypes = [ctypes.c_void_p, _dp]
+        L.gto_basis_shell_offsets.argtypes = [ctypes.c_void_p, _ip]
+        L.gto_overlap.argtypes = [ctypes.c_void_p, _dp]
+        L.gto_kinetic.argtypes = [ctypes.c_void_p, _dp]
+        L.gto_nuclear.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
+        L.gto_coulomb_2c.argtypes = [ctypes.c_void_p, _dp]
+        L.gto_coulomb_3c.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _dp]
+        L.gto_boys.argtypes = [ctypes.c_int, ctypes.c_double, _dp]
+        L.gto_set_threads.argtypes = [ctypes.c_int]
+        L.gto_set_threads.restype = None
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError("%s failed with code %d" % (what, rc))
+
+
+class Basis:
+    """A basis over a molecule's atoms (spherical shells unless pure=False)."""
+
+    def __init__(self, shells, pure=True):
+        self.shells = shells
+        l = np.array([s.l for s in shells], dtype=np.int32)
+        pu = np.full(len(shells), 1 if pure else 0, dtype=np.int32)
+        npr = np.array([len(s.exps) for s in shells], dtype=np.int32)
+        xyz = np.array([s.center for s in shells], dtype=np.float64).reshape(-1)
+        ex = np.array([e for s in shells for e in s.exps], dtype=np.float64)
+        co = np.array([c for s in shells for c in s.coefs], dtype=np.float64)
+        h = ctypes.c_void_p()
+        _check(lib().gto_basis_create(ctypes.byref(h), len(shells), _ptr(l, _ip), _ptr(pu, _ip), _ptr(npr, _ip),
+                                      _ptr(xyz), _ptr(ex), _ptr(co)), "gto_basis_create")
+        self._h = h
+        self.nbf = lib().gto_basis_nbf(h)
+        self.pure = pure
+
+    @classmethod
+    def for_molecule(cls, name, mol, pure=True):
+        return cls(_basis.build_shells(name, mol.symbols, mol.coords_bohr), pure=pure)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _LIB is not None:
+            _LIB.gto_basis_destroy(h)
+            self._h = None
+
+    def norm_coefs(self):
+        out = np.empty(sum(len(s.exps) for s in self.shells))
+        _check(lib().gto_basis_norm_coefs(self._h, _ptr(out)), "gto_basis_norm_coefs")
+        return out
+
+    def shell_offsets(self):
+        out = np.empty(len(self.shells), dtype=np.int32)
+        _check(lib().gto_basis_shell_offsets(self._h, _ptr(out, _ip)), "gto_basis_shell_offsets")
+        return out
+
+
+def overlap(b):
+    S = np.empty((b.nbf, b.nbf))
+    _check(lib().gto_overlap(b._h, _ptr(S)), "gto_overlap")
+    return S
+
+
+def kinetic(b):
+    T = np.empty((b.nbf, b.nbf))
+    _check(lib().gto_kinetic(b._h, _ptr(T)), "gto_kinetic")
+    return T
+
+
+def nuclear(b, mol):
+    V = np.empty((b.nbf, b.nbf))
+    Z = np.ascontiguousarray(mol.charges)
+    R = np.ascontiguousarray(mol.coords_bohr.reshape(-1))
+    _check(lib().gto_nuclear(b._h, len(Z), _ptr(Z), _ptr(R), _ptr(V)), "gto_nuclear")
+    return V
+
+
+def coulomb_2c(aux):
+    V = np.empty((aux.nbf, aux.nbf))
+    _check(lib().gto_coulomb_2c(aux._h, _ptr(V)), "gto_coulomb_2c")
+    return V
+
+
+def coulomb_3c(orb, aux, layout=LAYOUT_PACKED):
+    n, na = orb.nbf, aux.nbf
+    if layout == LAYOUT_NOPT_FULL:
+        out = np.empty((n * n, na))
+    else:
+        out = np.empty((n * (n + 1) // 2, na))
+    _check(lib().gto_coulomb_3c(orb._h, aux._h, layout, _ptr(out)), "gto_coulomb_3c")
+    return out
+
+
+def boys(mmax, T):
+    F = np.empty(mmax + 1)
+    _check(lib().gto_boys(mmax, T, _ptr(F)), "gto_boys")
+    return F
+
+
+def set_threads(n):
+    lib().gto_set_threads(int(n))
+
+
+class SystemIntegrals:
+    """All inputs of an RI-RHF calculation for one molecule."""
+
+    def __init__(self, mol, orb_basis, aux_basis, layout=LAYOUT_PACKED):
+        self.mol = mol
+        self.orb = Basis.for_molecule(orb_basis, mol)
+        self.aux = Basis.for_molecule(aux_basis, mol)
+        self.S = overlap(self.orb)
+        self.H = kinetic(self.orb) + nuclear(self.orb, mol)
+        self.V = coulomb_2c(self.aux)
+        self.layout = layout
+        self.I3 = coulomb_3c(self.orb, self.aux, layout)
+        self.Enuc = mol.nuclear_repulsion()
+        self.nocc = mol.nelec // 2
+
+    @property
+    def n(self):
+        return self.orb.nbf
+
+    @property
+    def naux(self):
+        return self.aux.nbf

@@ -1,0 +1,189 @@
+"""CPU oracle for the RI-JK Fock build — TEST INFRASTRUCTURE ONLY.
+
+This module is the checker.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg may import it; the product path (nopt_b200/, librijk.so) never does.
+
+It restates, in numpy (float64 throughout, OpenBLAS dgemm underneath), the reference's
+algorithm for the hot path in the reference's own operation order:
+
+  * DM_to_F_transform_RI          src/RI.cpp:115-176
+  * CASSCF inactive J/K tail      src/RI.cpp:235-287 (same algorithm, D_core / C_core)
+  * S05_calc  (metric V^-1/2)     src/matr.cpp:372-401
+  * gen_HF_DM (D = sum_i C_i C_i^T, normalised to 1)   src/SCF.cpp:63-73
+  * calc_F_AO (F = H + (2J - K) c, mc = 0/1/2)        src/molecule.cpp:4407-4438
+  * RHF energy E = tr(F D) + tr(H D) + V_nuc          src/SCF.cpp:134, E_1el_calc src/doCI_matr.cpp:38-47
+  * orbital gradient 4 F_ai                           src/converger_2_1.cpp:55-62
+
+Parity is pinned end to end: the RI-RHF energies this oracle reaches with the package's
+integral engine are checked against the reference's example logs
+(examples/c2h4_2_2/benchmark.log, examples/cis/benchmark.log) in tests/test_oracle_pins.py.
+"""
+import numpy as np
+
+
+# ------------------------------------------------------------------ metric ------
+def s05_calc(V):
+    """V^-1/2 and V^+1/2 as S05_calc (src/matr.cpp:372-401): eigendecomposition, eigenvalues
+    <= 0 dropped (the reference prints a warning and leaves the diagonal entry zero)."""
+    w, U = np.linalg.eigh(V)
+    m = np.zeros_like(w)
+    p = np.zeros_like(w)
+    pos = w > 0.0
+    p[pos] = np.sqrt(w[pos])
+    m[pos] = 1.0 / p[pos]
+    Vm05 = (U * m) @ U.T
+    Vp05 = (U * p) @ U.T
+    return Vm05, Vp05
+
+
+def cholesky_inverse_factor(V):
+    """L^-1 with V = L L^T (the Cholesky form of the metric; J and K agree with the V^-1/2
+    form in exact arithmetic since L^-T L^-1 = V^-1 = V^-1/2 V^-1/2)."""
+    L = np.linalg.cholesky(V)
+    return np.linalg.solve(L, np.eye(V.shape[0]))
+
+
+# --------------------------------------------------------------- RI tensors ------
+def unpack_3c(I3_packed, n):
+    """Packed (mu>=nu) three-centre array [(mu(mu+1)/2+nu), P] -> NOPT's RI_AA layout
+    [(mu*n+nu), P] (src/RI.cpp:69-71, src/libint_link.cpp:2320)."""
+    naux = I3_packed.shape[1]
+    full = np.empty((n, n, naux))
+    iu = np.tril_indices(n)
+    full[iu[0], iu[1]] = I3_packed
+    full[iu[1], iu[0]] = I3_packed
+    return full.reshape(n * n, naux)
+
+
+def dm_to_f_transform_ri(RI_AA, Vm05, DM, MO, n_c, n_ao):
+    """J, K exactly as DM_to_F_transform_RI (src/RI.cpp:115-176).
+
+    RI_AA: (n*n, naux) raw (mu nu|P), aux fastest.  Vm05: V^-1/2.  DM: n x n row-major
+    (not symmetrised).  MO: rows are orbitals (n_c rows used).  Returns (J, K), K unscaled.
+    """
+    naux = RI_AA.shape[1]
+    RI_J = DM.reshape(1, n_ao * n_ao) @ RI_AA            # :122-126  1 x naux
+    RI_J2 = Vm05 @ RI_J.reshape(naux, 1)                  # :128-132
+    RI_J = Vm05 @ RI_J2                                   # :134-138
+    J = (RI_AA @ RI_J).reshape(n_ao, n_ao)                # :140-144
+    MOc = np.ascontiguousarray(MO[:n_c])
+    RI_CA = MOc @ RI_AA.reshape(n_ao, n_ao * naux)        # :146-150  (i, nu, P)
+    RI_CA2 = RI_CA.reshape(n_c * n_ao, naux) @ Vm05       # :152-156
+    T = RI_CA2.reshape(n_c, n_ao, naux).transpose(1, 0, 2).reshape(n_ao, n_c * naux)  # :158-164
+    K = T @ T.T                                           # :167-171
+    return J, K
+
+
+def gen_hf_dm(MO, n, n_el):
+    """D[i,j] = sum_k MO[k,i] MO[k,j] over k < n_el (src/SCF.cpp:63-73)."""
+    C = MO[:n_el]
+    return C.T @ C
+
+
+def e_1el(X, DM):
+    """E_1el_calc (src/doCI_matr.cpp:38-47): sum_ij DM[i + n j] X[i n + j] = sum(DM^T * X)."""
+    return float(np.sum(DM.T * X))
+
+
+def calc_f_ao(H, J, K, c=1.0, mc=0):
+    """calc_F_AO (src/molecule.cpp:4418-4430)."""
+    if mc in (0, 2):
+        return H + (2.0 * J - K) * c
+    return H + (J - K) * (2.0 * c)
+
+
+def rhf_energy(F, H, DM, Enuc):
+    """E = tr(F D) + tr(H D) + V_nuc  (src/SCF.cpp:134)."""
+    return e_1el(F, DM) + e_1el(H, DM) + Enuc
+
+
+def orbital_gradient_max(F, MO, n_occ):
+    """max |4 F^MO_ai| (src/converger_2_1.cpp:55-62), F^MO = C F C^T (src/SCF.cpp:136-137)."""
+    Fmo = MO @ F @ MO.T
+    return float(np.max(np.abs(4.0 * Fmo[n_occ:, :n_occ]))) if Fmo.shape[0] > n_occ else 0.0
+
+
+# ------------------------------------------------------------ factored form ------
+def b_tensor(I3_packed, M):
+    """B^Q_{mu nu} = sum_P M_QP (P|mu nu) on the packed pair list: (npair, naux) -> (naux, npair)."""
+    return M @ I3_packed.T
+
+
+def jk_from_b(Bp, n, DM, MO, n_c):
+    """J, K from a packed fitted tensor B (naux x npair, mu>=nu).  Same quantities as
+    dm_to_f_transform_ri with B = V^-1/2 (P|mu nu); used at sizes where the full-square
+    RI_AA of the reference does not fit in host memory."""
+    naux = Bp.shape[0]
+    il = np.tril_indices(n)
+    Dsym = DM + DM.T
+    Dsym[np.diag_indices(n)] *= 0.5
+    w = Bp @ Dsym[il]
+    Jp = Bp.T @ w
+    J = np.zeros((n, n))
+    J[il] = Jp
+    J[il[1], il[0]] = Jp
+    C = np.ascontiguousarray(MO[:n_c])
+    K = np.zeros((n, n))
+    full = np.zeros((n, n))
+    for q in range(naux):
+        full[il] = Bp[q]
+        full[il[1], il[0]] = Bp[q]
+        X = C @ full
+        K += X.T @ X
+    return J, K
+
+
+# --------------------------------------------------------------------- SCF ------
+def scf_rhf(S, H, RI_AA, Vm05, n_occ, Enuc, conv_dm=1e-10, max_iter=100, diis_n=8, jk=None):
+    """Restricted HF with DIIS on F D S - S D F, using the reference's J/K, F and E
+    conventions.  Returns (E, MO, DM, F, iterations).  `jk(DM, MO) -> (J, K)` overrides the
+    Fock build (default: dm_to_f_transform_ri on RI_AA/Vm05)."""
+    n = S.shape[0]
+    s, U = np.linalg.eigh(S)
+    keep = s > 1e-10
+    X = U[:, keep] / np.sqrt(s[keep])
+    if jk is None:
+        jk = lambda D, MO: dm_to_f_transform_ri(RI_AA, Vm05, D, MO, n_occ, n)
+
+    def diag(F):
+        e, Cp = np.linalg.eigh(X.T @ F @ X)
+        return (X @ Cp).T  # rows are orbitals
+
+    MO = diag(H)
+    DM = gen_hf_dm(MO, n, n_occ)
+    focks, errs = [], []
+    E = 0.0
+    for it in range(1, max_iter + 1):
+        J, K = jk(DM, MO)
+        F = calc_f_ao(H, J, K)
+        E = rhf_energy(F, H, DM, Enuc)
+        err = X.T @ (F @ DM @ S - S @ DM @ F) @ X
+        focks.append(F)
+        errs.append(err)
+        if len(focks) > diis_n:
+            focks.pop(0)
+            errs.pop(0)
+        m = len(focks)
+        Bm = -np.ones((m + 1, m + 1))
+        Bm[m, m] = 0.0
+        for i in range(m):
+            for j in range(m):
+                Bm[i, j] = np.sum(errs[i] * errs[j])
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1.0
+        try:
+            coef = np.linalg.solve(Bm, rhs)[:m]
+        except np.linalg.LinAlgError:
+            coef = np.zeros(m)
+            coef[-1] = 1.0
+        Fd = sum(c * f for c, f in zip(coef, focks))
+        MO = diag(Fd)
+        DMn = gen_hf_dm(MO, n, n_occ)
+        rms = float(np.sqrt(np.mean((DMn - DM) ** 2)))
+        DM = DMn
+        if rms < conv_dm:
+            J, K = jk(DM, MO)
+            F = calc_f_ao(H, J, K)
+            E = rhf_energy(F, H, DM, Enuc)
+            return E, MO, DM, F, it
+    return E, MO, DM, F, max_iter
