@@ -1,0 +1,359 @@
+"""Benchmark of the RI-JK Fock build on B200: Fock builds per second.
+
+Workload (default): water 16-mer (H2O)16, cc-pVDZ / cc-pVDZ-JKFIT (n = 384, naux = 1856,
+nocc = 80), seeded jittered 4x2x2 lattice.  A step is one Fock build (J and K) over the
+resident fitted tensor B (1.3 GB, larger than the 126 MB L2, so no flush is needed between
+steps).  `value` is device-timed FP64 builds/s with the inputs in HBM; `e2e` is the same
+metric through the drop-in C ABI call (host D and C in, host J and K out); the mixed
+precision form and the SCF time to convergence are reported beside it.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the workload (the Fock
+build of one molecule is a one-GPU problem): weak scaling, value = total builds/s.
+`--impl reference` times the reference's CPU algorithm (the oracle's restatement of
+DM_to_F_transform_RI in the reference's dgemm order; the reference itself does not build
+here) on all host threads.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+METRIC = "RI-JK Fock builds/s (FP64 drop-in; mixed and SCF time beside it)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="h2o16_dz")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-scf", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def build_system(workload, seed):
+    from nopt_b200 import ints
+    from nopt_b200.molecules import WORKLOADS
+    fac, ob, ab = WORKLOADS[workload]
+    mol = fac(seed)
+    t = time.time()
+    si = ints.SystemIntegrals(mol, ob, ab, layout=ints.LAYOUT_PACKED)
+    return si, time.time() - t, (ob, ab)
+
+
+def core_guess(si):
+    """Orbitals of the core Hamiltonian (rows = orbitals), orthonormal in S."""
+    s, U = np.linalg.eigh(si.S)
+    X = U / np.sqrt(s)
+    e, Cp = np.linalg.eigh(X.T @ si.H @ X)
+    MO = (X @ Cp).T.copy()
+    DM = MO[:si.nocc].T @ MO[:si.nocc]
+    return DM, MO
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.lines, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_builds_per_s(si, DM, MO, budget_s):
+    """The oracle's restatement of DM_to_F_transform_RI on the host (all threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import rijk_oracle as O
+    from threadpoolctl import threadpool_info
+    RI = O.unpack_3c(si.I3, si.n)
+    Vm05, _ = O.s05_calc(si.V)
+    O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)  # warm
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)
+        k += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or k >= 50:
+            break
+    threads = max([p.get("num_threads", 1) for p in threadpool_info()] or [1])
+    return k / el, threads, "%d full builds in NOPT layout (RI_AA %.2f GB), %.1f s" % (k, RI.nbytes / 1e9, el)
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    si, tint, (ob, ab) = build_system(args.workload, args.seed)
+    DM, MO = core_guess(si)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import rijk_oracle as O
+    from threadpoolctl import threadpool_info
+    RI = O.unpack_3c(si.I3, si.n)
+    Vm05, _ = O.s05_calc(si.V)
+    for _ in range(max(args.warmup, 0)):
+        O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    threads = max([p.get("num_threads", 1) for p in threadpool_info()] or [1])
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "builds/s", "n_gpus": 0, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "(H2O)16 %s/%s" % (ob, ab), "n": si.n, "naux": si.naux, "nocc": si.nocc},
+           "cpu_baseline": {"value": v, "unit": "builds/s", "cores": threads, "kind": "port",
+                            "sample": "%d builds of the reference's dgemm sequence (oracle restatement; the reference "
+                                      "needs libint2/Eigen/Boost/LAPACKE, absent here)" % args.steps},
+           "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    from nopt_b200 import rijk
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    si, tint, (ob, ab) = build_system(args.workload, args.seed)
+    DM, MO = core_guess(si)
+    n, naux, nocc = si.n, si.naux, si.nocc
+    stream = torch.cuda.current_stream(dev)
+    fb = rijk.FockBuilder(local)
+    fb.set_stream(stream.cuda_stream)
+    fb.set_metric(si.V, rijk.METRIC_INVSQRT)
+    fb.set_3c(si.I3, n)
+    st0 = fb.stats()
+
+    dD = torch.from_numpy(DM).to(dev)
+    dMO = torch.from_numpy(MO[:nocc].copy()).to(dev)
+    dJ = torch.empty((n, n), dtype=torch.float64, device=dev)
+    dK = torch.empty((n, n), dtype=torch.float64, device=dev)
+
+    def timed(prec, steps, warm):
+        for _ in range(warm):
+            fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec)
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    with ClockSampler(local) as clk:
+        ms = timed(rijk.PREC_FP64, args.steps, max(args.warmup, 3))
+    st = fb.stats()
+    launches = st["kernels_last_fock"] * args.steps
+    value = world * 1e3 / ms
+
+    # end to end through the drop-in call: pinned host D, C in; host J, K out
+    hD = torch.from_numpy(DM).pin_memory()
+    hMO = torch.from_numpy(MO[:nocc].copy()).pin_memory()
+    hJ = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    hK = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    import ctypes
+    P = ctypes.POINTER(ctypes.c_double)
+    pD, pMO, pJ, pK = [ctypes.cast(t.data_ptr(), P) for t in (hD, hMO, hJ, hK)]
+    L = rijk.lib()
+    for _ in range(2):
+        fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+
+    # per-kernel device times (events around each launch on the launching stream)
+    fb.set_profiling(True)
+    stages = {}
+    for _ in range(5):
+        fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), rijk.PREC_FP64)
+        for k, v in fb.stats()["stages"].items():
+            stages.setdefault(k, []).append(v)
+    fb.set_profiling(False)
+    stage_ms = {k: float(np.median(v)) for k, v in stages.items()}
+    top = max(stage_ms, key=stage_ms.get)
+
+    peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    # FP64 peak: the box's own cuBLAS DGEMM (the driver's peak file has no FP64 figure)
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 1e9
+    for _ in range(3):
+        e0.record(stream)
+        torch.matmul(a, b)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1))
+    fp64_peak = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    del a, b
+    ntile, npad = st0["ntile"], st0["npad"]
+    noccp = (nocc + 15) // 16 * 16
+    tile_elems = ntile * 4096
+    algo = {
+        "coulomb_w": ("hbm", tile_elems * naux * 8.0),
+        "coulomb_j": ("hbm", tile_elems * naux * 8.0),
+        "xform_f64": ("tensor", 2.0 * noccp * npad * npad * naux),
+        "syrk_f64": ("tensor", float(npad) * (npad + 64) * noccp * naux),
+    }
+    kind, amount = algo.get(top, ("hbm", 0.0))
+    if kind == "hbm":
+        achieved = amount / (stage_ms[top] * 1e-3) / 1e9
+        roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+    else:
+        achieved = amount / (stage_ms[top] * 1e-3) / 1e12
+        roof = {"kernel": top, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "traffic": None,
+                "peak_source": "FP64 DMMA: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)"}
+    cw = stage_ms.get("coulomb_w", 0.0) + stage_ms.get("coulomb_j", 0.0)
+    coul = {"achieved_gbs": 2 * tile_elems * naux * 8.0 / (cw * 1e-3) / 1e9 if cw else None, "peak_gbs": hbm}
+    if coul["achieved_gbs"]:
+        coul["frac"] = coul["achieved_gbs"] / hbm
+
+    # mixed precision form, if built
+    mixed = None
+    try:
+        msm = timed(rijk.PREC_MIXED, args.steps, 3)
+        Jm, Km = dJ.cpu().numpy().copy(), dK.cpu().numpy().copy()
+        fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), rijk.PREC_FP64)
+        torch.cuda.synchronize(dev)
+        mixed = {"value": world * 1e3 / msm, "ms_per_step": msm, "speedup_vs_fp64": ms / msm,
+                 "max_abs_dK_vs_fp64": float(np.max(np.abs(Km - dK.cpu().numpy())))}
+    except rijk.RijkError as e:
+        mixed = {"unavailable": str(e)}
+
+    # SCF to convergence with every Fock build on the GPU
+    scf = None
+    if not args.no_scf and rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import rijk_oracle as O  # noqa: F401  (only its SCF driver loop is used here)
+        t0 = time.perf_counter()
+        jk = lambda D, C: fb.dm_to_f_transform_ri(D, C, nocc)
+        E, _, _, _, it = O.scf_rhf(si.S, si.H, None, None, nocc, si.Enuc, jk=jk)
+        scf = {"seconds": time.perf_counter() - t0, "iterations": it, "energy": E,
+               "driver": "host DIIS loop, GPU Fock builds (FP64)"}
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        v, threads, sample = cpu_builds_per_s(si, DM, MO, args.cpu_seconds)
+        cpu = {"value": v, "unit": "builds/s", "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
+               "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": "(H2O)16 %s/%s" % (ob, ab) if args.workload == "h2o16_dz" else args.workload,
+                          "n": n, "naux": naux, "nocc": nocc, "parallelism": "replicas" if world > 1 else "single",
+                          "l2": "inputs larger than L2 (B = %.2f GB)" % (st0["bytes_b"] / 1e9),
+                          "seed": args.seed},
+               "e2e": {"value": world * 1e3 / ms_e2e, "unit": "builds/s",
+                       "h2d_bytes_per_step": int((n * n + nocc * n) * 8), "d2h_bytes_per_step": int(2 * n * n * 8)},
+               "gpu_launches": launches,
+               "roofline": roof, "coulomb_roofline": coul, "stage_ms": stage_ms,
+               "mixed": mixed, "scf": scf, "cpu_baseline": cpu, "clocks": clk.summary(),
+               "setup": {"integrals_s": tint, "metric_ms": st0["ms_setup_metric"], "b_ms": st0["ms_setup_3c"]}}
+        print(json.dumps(out), flush=True)
+    fb.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,105 @@
+/*
+ * rijk.h — C ABI of the B200 RI-JK Fock build (librijk.so).
+ *
+ * Drop-in for the reference's RI Fock-build routine and its set-up:
+ *   rijk_set_metric   replaces RI_V_calc + S05_calc        src/libint_link.cpp:2049-2107, src/matr.cpp:372-401
+ *   rijk_set_3c       replaces the RI_AA set-up of gen_RI_AA / regen_RI_AA
+ *                                                          src/RI.cpp:34-101 (consumer of calc_2el_AO_INTS_RI,
+ *                                                          src/libint_link.cpp:2261-2350)
+ *   rijk_fock         replaces DM_to_F_transform_RI        src/RI.cpp:115-176 (declared include/RI.h)
+ *                     and the J/K tail of calc_2el_MO_INTS_RI  src/RI.cpp:235-287
+ *   rijk_fock_energy  F = H + (2J - K) c and the RHF energy   src/molecule.cpp:4407-4438, src/SCF.cpp:134
+ *   rijk_scf          the RHF loop around it (DIIS variant)   src/SCF.cpp:78-223
+ *   rijk_grad         adjoint of the Fock build (no reference counterpart: the reference
+ *                     differentiates by finite differences, src/QM_calc.cpp:142)
+ *
+ * Conventions are the reference's: all matrices are host (or, for *_device calls, device)
+ * double arrays in row-major order; D is normalised to 1 (D = sum_i C_i C_i^T over occupied
+ * rows of MO, src/SCF.cpp:63-73) and is used as given (not symmetrised); MO holds one
+ * orbital per row (n_c rows of n_ao); K is unscaled; J and K are full n x n.
+ *
+ * One context drives one GPU.  A context is not thread-safe.  Every function returns
+ * RIJK_OK (0) or a negative RIJK_ERR_* code; rijk_last_error() gives the message.  Nothing
+ * in the library calls exit() or aborts.
+ */
+#ifndef RIJK_H
+#define RIJK_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RIJK_OK 0
+#define RIJK_ERR_ARG -1      /* null pointer, bad size or bad enum value                      */
+#define RIJK_ERR_STATE -2    /* call order (e.g. rijk_fock before rijk_set_3c)                */
+#define RIJK_ERR_CUDA -3     /* CUDA runtime error                                             */
+#define RIJK_ERR_ALLOC -4    /* device memory exhausted                                        */
+#define RIJK_ERR_SOLVER -5   /* metric factorisation failed (e.g. not positive definite)       */
+#define RIJK_ERR_TIMEOUT -6  /* a bounded device-side wait ran out                             */
+#define RIJK_ERR_NUMERIC -7  /* NaN or Inf met in an input or a result                        */
+#define RIJK_ERR_CONVERGE -8 /* SCF did not converge within the iteration limit                */
+
+/* Metric forms.  J and K agree in exact arithmetic (L^-T L^-1 = V^-1 = V^-1/2 V^-1/2). */
+#define RIJK_METRIC_INVSQRT 0  /* V^-1/2 by eigendecomposition, eigenvalues <= 0 dropped (S05_calc) */
+#define RIJK_METRIC_CHOLESKY 1 /* L^-1 with V = L L^T                                               */
+
+/* Layouts of the three-centre integrals handed to rijk_set_3c. */
+#define RIJK_LAYOUT_NOPT_FULL 0 /* I3[(mu*n + nu)*naux + P], full square: the reference's RI_AA */
+#define RIJK_LAYOUT_PACKED 1    /* I3[(mu*(mu+1)/2 + nu)*naux + P], mu >= nu                    */
+
+/* Arithmetic of one Fock build. */
+#define RIJK_PREC_FP64 0  /* FP64 throughout: the drop-in form                                   */
+#define RIJK_PREC_MIXED 1 /* exchange half-transform and K on tcgen05 tensor cores with split-BF16
+                             (3-term) operands and FP32 accumulation; Coulomb in FP64          */
+
+typedef struct rijk_ctx rijk_ctx;
+
+typedef struct {
+  double ms_setup_metric; /* last rijk_set_metric, device time                             */
+  double ms_setup_3c;     /* last rijk_set_3c, device time (metric contraction included)   */
+  double ms_last_fock;    /* last Fock build, device time                                   */
+  double ms_coulomb;      /* of which the Coulomb pair (w and J passes)                     */
+  double ms_exchange;     /* of which half-transform + K                                    */
+  double flops_last_fock; /* algorithmic FLOPs of the last build                            */
+  double bytes_last_fock; /* algorithmic HBM bytes of the last build                        */
+  long n, naux, npad, ntile;
+  long bytes_b;           /* device bytes of the fitted tensor B                            */
+  long bytes_b_mixed;     /* device bytes of its split-BF16 copy (0 until first mixed build) */
+  int kernels_last_fock;  /* kernels launched by the last build                             */
+  int profiled_stages;    /* number of valid entries of ms_stage (0 unless profiling is on)  */
+  double ms_stage[12];    /* device time of each kernel of the last build, in launch order   */
+  char stage_names[12][24];
+} rijk_stats_t;
+
+int rijk_create(rijk_ctx** ctx, int device);
+int rijk_destroy(rijk_ctx* ctx);
+/* Run on the caller's CUDA stream (a cudaStream_t) instead of the context's own. */
+int rijk_set_stream(rijk_ctx* ctx, void* stream);
+int rijk_last_error(const rijk_ctx* ctx, char* buf, int len);
+/* Record a CUDA event around every kernel of a Fock build (for per-kernel timing). */
+int rijk_set_profiling(rijk_ctx* ctx, int on);
+int rijk_get_stats(const rijk_ctx* ctx, rijk_stats_t* out);
+
+/* (P|Q), naux x naux host array.  Factorises the metric on the GPU in FP64. */
+int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int metric_form);
+
+/* Three-centre integrals (host array, layout RIJK_LAYOUT_*).  Forms the fitted tensor
+ * B^Q_{mu nu} = sum_P M_QP (P|mu nu) on the GPU, stored packed (mu >= nu) in HBM. */
+int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n_ao, long naux, int layout);
+
+/* Drop-in for DM_to_F_transform_RI(J, K, DM, MO, n_c, n_ao): host pointers, synchronous. */
+int rijk_fock(rijk_ctx* ctx, const double* DM, const double* MO, long n_c, double* J, double* K, int precision);
+
+/* Same on device pointers, asynchronous on the context's stream. */
+int rijk_fock_device(rijk_ctx* ctx, const double* dDM, const double* dMO, long n_c, double* dJ, double* dK,
+                     int precision);
+
+/* F = H + (2J - K) c (mc = 0/2) or H + (J - K) 2c (mc = 1), src/molecule.cpp:4418-4430, and
+ * E = tr(F D) + tr(H D) + e_nuc (src/SCF.cpp:134); host pointers; F or E may be NULL. */
+int rijk_fock_energy(rijk_ctx* ctx, const double* H, const double* DM, const double* J, const double* K, double c,
+                     int mc, double e_nuc, double* F, double* E);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

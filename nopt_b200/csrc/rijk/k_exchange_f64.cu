@@ -1,0 +1,215 @@
+// k_exchange_f64.cu — FP64 exchange: half-transform (K3) and K contraction (K4).
+//
+// Reference (src/RI.cpp:146-171): RI_CA = MO . RI_AA (i, nu, P), RI_CA2 = RI_CA . V^-1/2,
+// transpose to (nu, i, P), K = RI_CA RI_CA^T over (i, P).  With the metric folded into B:
+//
+//   K3  XT[nu][Q*noccp + i] = sum_mu B^Q_{nu mu} C_{i mu}
+//       one CTA per (nu-block J, Q); the mu loop walks the stored tiles (J, I) for I <= J
+//       and the transposes of (I, J) for I > J, so B's packed triangle is read as the full
+//       symmetric matrix without unpacking.
+//   K4  K[mu][nu] = sum_k XT[mu][k] XT[nu][k], k = (Q, i): only the lower tiles (a >= b)
+//       are formed, split over k into nsplit ranges whose partial tiles are summed (and
+//       mirrored) by the unpack kernel.  FLOPs n(n+1) noccp naux, the SYRK count.
+#include "gemm_f64.cuh"
+#include "rijk_internal.h"
+
+namespace rijk {
+
+constexpr int X_THREADS = 128;
+
+template <int NF>
+__global__ void __launch_bounds__(X_THREADS)
+    k_xform_f64(const double* __restrict__ B, const double* __restrict__ MOp, long nt, long npad, long tile_elems,
+                long kdim, double* __restrict__ XT) {
+  constexpr int NOCCP = NF * 16;
+  constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
+  constexpr int B_STAGE = NOCCP * LDK;
+  extern __shared__ __align__(16) double smem[];
+  double* sA[2] = {smem, smem + A_STAGE};
+  double* sB[2] = {smem + 2 * A_STAGE, smem + 2 * A_STAGE + B_STAGE};
+
+  const long J = blockIdx.x;
+  const long Q = blockIdx.y;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const double* BQ = B + Q * tile_elems;
+
+  auto load = [&](int stage, long kc) {
+    const long I = kc >> 1;
+    const int half = static_cast<int>(kc & 1);
+    if (J >= I) {  // tile (J, I): rows nu, cols mu -> [nu][mu-chunk]
+      const double* tp = BQ + tri_index(J, I) * TILE2 + half * KC;
+#pragma unroll
+      for (int it = 0; it < 8; ++it) {
+        int idx = tid + it * X_THREADS;
+        int row = idx >> 4, seg = idx & 15;
+        cp_async16(&sA[stage][row * LDK + seg * 2], tp + row * TILE + seg * 2, true);
+      }
+    } else {  // tile (I, J): rows mu, cols nu -> [mu-chunk][nu]
+      const double* tp = BQ + tri_index(I, J) * TILE2 + half * KC * TILE;
+#pragma unroll
+      for (int it = 0; it < 8; ++it) {
+        int idx = tid + it * X_THREADS;
+        int row = idx >> 5, seg = idx & 31;
+        cp_async16(&sA[stage][row * LDM + seg * 2], tp + row * TILE + seg * 2, true);
+      }
+    }
+    const double* cp = MOp + I * TILE + half * KC;
+    for (int idx = tid; idx < NOCCP * 16; idx += X_THREADS) {
+      int row = idx >> 4, seg = idx & 15;
+      cp_async16(&sB[stage][row * LDK + seg * 2], cp + row * npad + seg * 2, true);
+    }
+  };
+
+  double acc[4][NF][2];
+  zero_acc(acc);
+  const long nk = nt * 2;
+  load(0, 0);
+  cp_async_commit();
+  for (long kc = 0; kc < nk; ++kc) {
+    if (kc + 1 < nk) {
+      load(static_cast<int>((kc + 1) & 1), kc + 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    if (J >= (kc >> 1))
+      warp_mma_chunk<4, NF, true>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * (NOCCP / 2), lane);
+    else
+      warp_mma_chunk<4, NF, false>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * (NOCCP / 2), lane);
+    __syncthreads();
+  }
+
+  const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    long nu = J * TILE + wm * 32 + i * 8 + g;
+    double* row = XT + nu * kdim + Q * NOCCP + wn * (NOCCP / 2);
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+      *reinterpret_cast<double2*>(row + j * 8 + 2 * tq) = make_double2(acc[i][j][0], acc[i][j][1]);
+  }
+}
+
+template <int NF>
+static void launch_xform_nf(const double* B, const double* MOp, long naux, long nt, double* XT, cudaStream_t s) {
+  constexpr int NOCCP = NF * 16;
+  constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
+  size_t smem = (2 * A_STAGE + 2 * NOCCP * LDK) * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_xform_f64<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    attr = true;
+  }
+  long npad = nt * TILE;
+  long tile_elems = nt * (nt + 1) / 2 * TILE2;
+  dim3 grid(static_cast<unsigned>(nt), static_cast<unsigned>(naux));
+  k_xform_f64<NF><<<grid, X_THREADS, smem, s>>>(B, MOp, nt, npad, tile_elems, naux * NOCCP, XT);
+}
+
+void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s) {
+  switch (noccp / 16) {
+    case 1: launch_xform_nf<1>(B, MOp, naux, nt, XT, s); break;
+    case 2: launch_xform_nf<2>(B, MOp, naux, nt, XT, s); break;
+    case 3: launch_xform_nf<3>(B, MOp, naux, nt, XT, s); break;
+    case 4: launch_xform_nf<4>(B, MOp, naux, nt, XT, s); break;
+    case 5: launch_xform_nf<5>(B, MOp, naux, nt, XT, s); break;
+    case 6: launch_xform_nf<6>(B, MOp, naux, nt, XT, s); break;
+    case 7: launch_xform_nf<7>(B, MOp, naux, nt, XT, s); break;
+    case 8: launch_xform_nf<8>(B, MOp, naux, nt, XT, s); break;
+    case 9: launch_xform_nf<9>(B, MOp, naux, nt, XT, s); break;
+    case 10: launch_xform_nf<10>(B, MOp, naux, nt, XT, s); break;
+    case 11: launch_xform_nf<11>(B, MOp, naux, nt, XT, s); break;
+    case 12: launch_xform_nf<12>(B, MOp, naux, nt, XT, s); break;
+    default: break;  // rejected by the API (n_c > 192)
+  }
+}
+
+constexpr int S_THREADS = 128;
+
+__global__ void __launch_bounds__(S_THREADS)
+    k_syrk_f64(const double* __restrict__ XT, long kdim, long kper, long ntile, double* __restrict__ Kpart) {
+  extern __shared__ __align__(16) double smem_s[];
+  double* sA[2] = {smem_s, smem_s + 64 * LDK};
+  double* sB[2] = {smem_s + 2 * 64 * LDK, smem_s + 3 * 64 * LDK};
+  const long t = blockIdx.x;
+  const long s = blockIdx.y;
+  long a, b;
+  tri_decode(t, a, b);
+  const long k0 = s * kper;
+  const long k1 = k0 + kper < kdim ? k0 + kper : kdim;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const double* Ar = XT + a * TILE * kdim;
+  const double* Br = XT + b * TILE * kdim;
+
+  auto load = [&](int stage, long kk) {
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+      int idx = tid + it * S_THREADS;
+      int row = idx >> 4, seg = idx & 15;
+      long k = kk + seg * 2;
+      bool ok = k < k1;
+      cp_async16(&sA[stage][row * LDK + seg * 2], ok ? Ar + row * kdim + k : XT, ok);
+      cp_async16(&sB[stage][row * LDK + seg * 2], ok ? Br + row * kdim + k : XT, ok);
+    }
+  };
+
+  double acc[4][4][2];
+  zero_acc(acc);
+  const long nk = k1 > k0 ? (k1 - k0 + KC - 1) / KC : 0;
+  if (nk > 0) {
+    load(0, k0);
+    cp_async_commit();
+  }
+  for (long kc = 0; kc < nk; ++kc) {
+    if (kc + 1 < nk) {
+      load(static_cast<int>((kc + 1) & 1), k0 + (kc + 1) * KC);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    warp_mma_chunk<4, 4, true>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * 32, lane);
+    __syncthreads();
+  }
+  const int g = lane >> 2, tq = lane & 3;
+  double* out = Kpart + (s * ntile + t) * TILE2;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int r = wm * 32 + i * 8 + g;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int c = wn * 32 + j * 8 + 2 * tq;
+      *reinterpret_cast<double2*>(out + r * TILE + c) = make_double2(acc[i][j][0], acc[i][j][1]);
+    }
+  }
+}
+
+int syrk_nsplit(long nt, long kdim) {
+  long ntile = nt * (nt + 1) / 2;
+  long want = (148L * 4 + ntile - 1) / ntile;
+  long maxs = kdim / (KC * 8);
+  if (want > maxs) want = maxs;
+  if (want < 1) want = 1;
+  return static_cast<int>(want);
+}
+
+void launch_syrk_f64(const double* XT, long npad, long nt, long kdim, int nsplit, double* Kpart, cudaStream_t s) {
+  (void)npad;
+  long ntile = nt * (nt + 1) / 2;
+  long kper = round_up((kdim + nsplit - 1) / nsplit, KC);
+  dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(nsplit));
+  const size_t smem = 4 * 64 * LDK * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_syrk_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    attr = true;
+  }
+  k_syrk_f64<<<grid, S_THREADS, smem, s>>>(XT, kdim, kper, ntile, Kpart);
+}
+
+}  // namespace rijk

@@ -1,0 +1,107 @@
+// rijk_internal.h — context, device layout and kernel launchers of librijk.
+//
+// Device layout of the fitted tensor (the reference keeps the raw full square
+// RI_AA[(mu*n+nu)*naux+P] in host RAM, src/RI.cpp:69-71; here B already carries the metric
+// and only the lower triangle is stored):
+//
+//   n      orbital functions, npad = n rounded up to TILE (64), nt = npad / TILE
+//   tiles  the lower block triangle, tile (I, J) with I >= J at index I(I+1)/2 + J,
+//          each a dense TILE x TILE row-major block: element (r, c) is (mu, nu) =
+//          (I*TILE + r, J*TILE + c).  Diagonal tiles hold both triangles; padding is zero.
+//   B      double [naux][ntile][TILE][TILE]   (Q-major: one aux function's tensor is contiguous)
+//
+// Exchange intermediate (FP64 form): XT[nu][Q*noccp + i] = sum_mu C_{mu i} B^Q_{mu nu}, the
+// half-transformed tensor with the contraction index k = (Q, i) contiguous.
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cstdint>
+#include <string>
+
+#include "rijk.h"
+
+namespace rijk {
+
+constexpr int TILE = 64;
+constexpr int TILE2 = TILE * TILE;
+
+inline long round_up(long x, long m) { return (x + m - 1) / m * m; }
+
+// Device-side error word bits (written by kernels instead of trapping).
+constexpr int DEVERR_TIMEOUT = 1;
+constexpr int DEVERR_NAN = 2;
+constexpr int DEVERR_BOUNDS = 4;
+
+struct DeviceBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace rijk
+
+struct rijk_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+
+  long n = 0, naux = 0, npad = 0, nt = 0, ntile = 0;
+  int metric_form = RIJK_METRIC_INVSQRT;
+  bool have_metric = false, have_b = false;
+
+  rijk::DeviceBuf M;      // metric factor, naux x naux
+  rijk::DeviceBuf B;      // fitted tensor, naux x ntile x TILE2 doubles
+  rijk::DeviceBuf Bmix;   // split-BF16 copy of B for the mixed form (hi/lo planes)
+  bool have_bmix = false;
+  rijk::DeviceBuf stageD, stageMO, stageJ, stageK;  // n x n, n_c x n staging for host calls
+  rijk::DeviceBuf Dt;     // packed density weights, ntile x TILE2
+  rijk::DeviceBuf w;      // naux
+  rijk::DeviceBuf Jpart;  // Coulomb partials, nsplit x ntile x TILE2
+  rijk::DeviceBuf MOp;    // padded occupied coefficients, noccp x npad
+  rijk::DeviceBuf XT;     // half-transformed tensor
+  rijk::DeviceBuf Kpart;  // exchange split-K partials
+  rijk::DeviceBuf err;    // int device error word
+  rijk::DeviceBuf scratch;  // misc small
+
+  rijk_stats_t stats{};
+  std::string last_error;
+
+  // per-kernel timing (rijk_set_profiling)
+  bool profiling = false;
+  cudaEvent_t pev[13] = {};
+  int npev = 0;
+  const char* pname[12] = {};
+};
+
+namespace rijk {
+
+// Marks the end of one kernel when profiling is on (first call marks the start).
+void prof_mark(rijk_ctx* ctx, const char* name);
+
+// ---- k_pack.cu
+void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);
+void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s);
+void launch_unpack_sym(const double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s);
+void launch_scan_nonfinite(const double* x, long count, int* err, cudaStream_t s);
+
+// ---- k_metric.cu
+// B[Q][tile-packed e] = sum_P M[Q][P] * I3(pair(e), P) for the raw rows of tile rows [I0, I1).
+void launch_metric_contract_chunk(const double* M, long nauxp, const double* I3, int layout, long n, long naux,
+                                  long nt, long I0, long I1, double* B, cudaStream_t s);
+
+// ---- k_coulomb.cu
+int coulomb_nsplit(long tile_elems, long naux);
+void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s);
+void launch_coulomb_j(const double* B, const double* w, long naux, long tile_elems, int nsplit, double* Jpart,
+                      cudaStream_t s);
+
+// ---- k_exchange_f64.cu
+void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s);
+int syrk_nsplit(long nt, long kdim);
+void launch_syrk_f64(const double* XT, long npad, long nt, long kdim, int nsplit, double* Kpart, cudaStream_t s);
+
+}  // namespace rijk

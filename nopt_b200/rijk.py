@@ -1,0 +1,166 @@
+"""Python binding of librijk.so (include/rijk.h), the B200 RI-JK Fock build.
+
+The methods mirror the reference's RI interface (include/RI.h of the reference):
+
+  FockBuilder.set_metric          RI_V_calc + S05_calc        src/libint_link.cpp:2049, src/matr.cpp:372
+  FockBuilder.set_3c              RI_AA set-up of gen_RI_AA   src/RI.cpp:34-79
+  FockBuilder.dm_to_f_transform_ri  DM_to_F_transform_RI      src/RI.cpp:115-176
+  FockBuilder.calc_f_ao           F and E of calc_F_AO / RHF  src/molecule.cpp:4407-4438, src/SCF.cpp:134
+
+Errors raise RijkError carrying the library's status code and message; there is no
+fallback path: if librijk.so is missing the import of this module's functions fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+OK = 0
+ERR_ARG, ERR_STATE, ERR_CUDA, ERR_ALLOC, ERR_SOLVER, ERR_TIMEOUT, ERR_NUMERIC, ERR_CONVERGE = -1, -2, -3, -4, -5, -6, -7, -8
+METRIC_INVSQRT, METRIC_CHOLESKY = 0, 1
+LAYOUT_NOPT_FULL, LAYOUT_PACKED = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("ms_setup_metric", ctypes.c_double), ("ms_setup_3c", ctypes.c_double),
+                ("ms_last_fock", ctypes.c_double), ("ms_coulomb", ctypes.c_double),
+                ("ms_exchange", ctypes.c_double), ("flops_last_fock", ctypes.c_double),
+                ("bytes_last_fock", ctypes.c_double), ("n", ctypes.c_long), ("naux", ctypes.c_long),
+                ("npad", ctypes.c_long), ("ntile", ctypes.c_long), ("bytes_b", ctypes.c_long),
+                ("bytes_b_mixed", ctypes.c_long), ("kernels_last_fock", ctypes.c_int),
+                ("profiled_stages", ctypes.c_int), ("ms_stage", ctypes.c_double * 12),
+                ("stage_names", (ctypes.c_char * 24) * 12)]
+
+
+class RijkError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("rijk error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib_path():
+    return os.path.join(_HERE, "librijk.so")
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise RuntimeError("librijk.so is not built (run __graft_entry__.build()); there is no CPU fallback")
+        L = ctypes.CDLL(path)
+        P = ctypes.POINTER
+        L.rijk_create.argtypes = [P(_vp), ctypes.c_int]
+        L.rijk_destroy.argtypes = [_vp]
+        L.rijk_set_stream.argtypes = [_vp, _vp]
+        L.rijk_last_error.argtypes = [_vp, ctypes.c_char_p, ctypes.c_int]
+        L.rijk_get_stats.argtypes = [_vp, P(Stats)]
+        L.rijk_set_profiling.argtypes = [_vp, ctypes.c_int]
+        L.rijk_set_metric.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_int]
+        L.rijk_set_3c.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_int]
+        L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
+        L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
+        L.rijk_fock_energy.argtypes = [_vp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, _dp]
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class FockBuilder:
+    """One GPU context holding the fitted tensor B in HBM."""
+
+    def __init__(self, device=0):
+        h = _vp()
+        rc = lib().rijk_create(ctypes.byref(h), int(device))
+        if rc != OK:
+            raise RijkError(rc, "rijk_create(device=%d) failed" % device)
+        self._h = h
+        self.n = self.naux = None
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().rijk_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != OK:
+            buf = ctypes.create_string_buffer(512)
+            lib().rijk_last_error(self._h, buf, 512)
+            raise RijkError(rc, buf.value.decode())
+
+    def last_error(self):
+        buf = ctypes.create_string_buffer(512)
+        lib().rijk_last_error(self._h, buf, 512)
+        return buf.value.decode()
+
+    def set_stream(self, stream_ptr):
+        self._check(lib().rijk_set_stream(self._h, _vp(int(stream_ptr))))
+
+    def set_metric(self, V, form=METRIC_INVSQRT):
+        V = _c(V)
+        self._check(lib().rijk_set_metric(self._h, _p(V), V.shape[0], form))
+        self.naux = V.shape[0]
+
+    def set_3c(self, I3, n, layout=LAYOUT_PACKED):
+        I3 = _c(I3)
+        self._check(lib().rijk_set_3c(self._h, _p(I3), int(n), I3.shape[-1], layout))
+        self.n = n
+
+    def dm_to_f_transform_ri(self, DM, MO, n_c, precision=PREC_FP64, J=None, K=None):
+        """(J, K) exactly as the reference's DM_to_F_transform_RI(J, K, DM, MO, n_c, n_ao)."""
+        n = self.n
+        DM = _c(DM)
+        MO = _c(MO) if n_c > 0 else np.zeros((1, n))
+        J = np.empty((n, n)) if J is None else J
+        K = np.empty((n, n)) if K is None else K
+        self._check(lib().rijk_fock(self._h, _p(DM), _p(MO), int(n_c), _p(J), _p(K), precision))
+        return J, K
+
+    def fock_device(self, dD, dMO, n_c, dJ, dK, precision=PREC_FP64):
+        """Device-pointer form (ints from tensor.data_ptr()), asynchronous on the context stream."""
+        self._check(lib().rijk_fock_device(self._h, _vp(dD), _vp(dMO), int(n_c), _vp(dJ), _vp(dK), precision))
+
+    def calc_f_ao(self, H, DM, J, K, c=1.0, mc=0, e_nuc=0.0):
+        n = self.n
+        F = np.empty((n, n))
+        E = ctypes.c_double(0.0)
+        self._check(lib().rijk_fock_energy(self._h, _p(_c(H)), _p(_c(DM)), _p(_c(J)), _p(_c(K)), c, mc, e_nuc,
+                                           _p(F), ctypes.byref(E)))
+        return F, E.value
+
+    def set_profiling(self, on):
+        self._check(lib().rijk_set_profiling(self._h, 1 if on else 0))
+
+    def stats(self):
+        s = Stats()
+        self._check(lib().rijk_get_stats(self._h, ctypes.byref(s)))
+        out = {k: getattr(s, k) for k, _ in Stats._fields_ if k not in ("ms_stage", "stage_names")}
+        k = s.profiled_stages
+        out["stages"] = {s.stage_names[i].value.decode(): s.ms_stage[i] for i in range(k)}
+        return out
