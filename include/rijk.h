@@ -94,6 +94,24 @@ int rijk_fock(rijk_ctx* ctx, const double* DM, const double* MO, long n_c, doubl
 int rijk_fock_device(rijk_ctx* ctx, const double* dDM, const double* dMO, long n_c, double* dJ, double* dK,
                      int precision);
 
+/* Size of the fixed device scratch used by rijk_coulomb_noalloc (per GPU, held until exit). */
+#define RIJK_NOALLOC_SCRATCH_BYTES (32L * 1024 * 1024)
+
+/* No counterpart in the reference.  The Coulomb matrix J of rijk_fock_device, computed
+ * without any device allocation.  It is for callers that cannot let the library call
+ * cudaMalloc while their iterations run, for example a program that hands all of its GPU
+ * memory to its own pool at start-up, or one that must not add an allocation (and the
+ * device synchronisation it may bring) inside its loop.  The fitted tensor set up by
+ * rijk_set_3c is the input; dDM (n x n) and dJ (n x n) are device pointers of the caller;
+ * the call is asynchronous on the context's stream.  Working space comes from a fixed
+ * RIJK_NOALLOC_SCRATCH_BYTES device array inside the library:
+ *  - sizes that need more return RIJK_ERR_ARG (about n_ao <= 1980 fits);
+ *  - all calls on one GPU share it, so calls that overlap on the GPU race;
+ *  - the first call on each device looks up the array's address and should come before any
+ *    stream capture.
+ * The call makes no cudaMalloc, cudaFree or allocating library call. */
+int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ);
+
 /* F = H + (2J - K) c (mc = 0/2) or H + (J - K) 2c (mc = 1), src/molecule.cpp:4418-4430, and
  * E = tr(F D) + tr(H D) + e_nuc (src/SCF.cpp:134); host pointers; F or E may be NULL. */
 int rijk_fock_energy(rijk_ctx* ctx, const double* H, const double* DM, const double* J, const double* K, double c,
