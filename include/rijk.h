@@ -94,6 +94,10 @@ int rijk_fock(rijk_ctx* ctx, const double* DM, const double* MO, long n_c, doubl
 int rijk_fock_device(rijk_ctx* ctx, const double* dDM, const double* dMO, long n_c, double* dJ, double* dK,
                      int precision);
 
+/* Wait for the context's stream and report any error a kernel raised (RIJK_ERR_TIMEOUT when
+ * a bounded device-side wait ran out); also refreshes the timing statistics. */
+int rijk_sync(rijk_ctx* ctx);
+
 /* Size of the fixed device scratch used by rijk_coulomb_noalloc (per GPU, held until exit). */
 #define RIJK_NOALLOC_SCRATCH_BYTES (32L * 1024 * 1024)
 

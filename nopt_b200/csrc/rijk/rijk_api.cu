@@ -477,6 +477,31 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
   return RIJK_OK;
 }
 
+// Reads and clears the device error word the kernels raise instead of trapping.
+static int check_device_error(rijk_ctx* ctx) {
+  int h = 0;
+  int rc = cuda_check(ctx, cudaMemcpy(&h, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+  if (rc) return rc;
+  if (h == 0) return RIJK_OK;
+  cudaMemset(ctx->err.p, 0, sizeof(int));
+  if (h & DEVERR_TIMEOUT) return set_err(ctx, RIJK_ERR_TIMEOUT, "a device-side wait ran out (error bits 0x%x)", h);
+  if (h & DEVERR_NAN) return set_err(ctx, RIJK_ERR_NUMERIC, "non-finite value detected (error bits 0x%x)", h);
+  return set_err(ctx, RIJK_ERR_CUDA, "device error bits 0x%x", h);
+}
+
+RIJK_API int rijk_sync(rijk_ctx* ctx) {
+  if (!ctx) return RIJK_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "rijk_sync");
+  if (rc) return rc;
+  rc = check_device_error(ctx);
+  if (rc) return rc;
+  ctx->stats.ms_coulomb = elapsed(ctx->ev0, ctx->ev1);
+  ctx->stats.ms_exchange = elapsed(ctx->ev1, ctx->ev2);
+  ctx->stats.ms_last_fock = elapsed(ctx->ev0, ctx->ev2);
+  return RIJK_OK;
+}
+
 static int check_fock_args(rijk_ctx* ctx, long nocc, int precision) {
   if (!ctx->have_b) return set_err(ctx, RIJK_ERR_STATE, "Fock build before rijk_set_3c");
   if (nocc < 0 || nocc > ctx->n) return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld outside [0, n_ao = %ld]", nocc, ctx->n);
@@ -521,6 +546,7 @@ RIJK_API int rijk_fock(rijk_ctx* ctx, const double* D, const double* MO, long no
   rc = cuda_check(ctx, cudaMemcpyAsync(J, ctx->stageJ.p, nn, cudaMemcpyDeviceToHost, s), "D2H J");
   if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(K, ctx->stageK.p, nn, cudaMemcpyDeviceToHost, s), "D2H K");
   if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_fock");
+  if (!rc) rc = check_device_error(ctx);
   if (rc) return rc;
   ctx->stats.ms_coulomb = elapsed(ctx->ev0, ctx->ev1);
   ctx->stats.ms_exchange = elapsed(ctx->ev1, ctx->ev2);

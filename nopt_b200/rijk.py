@@ -67,6 +67,7 @@ def lib():
         L.rijk_set_3c.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_int]
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
+        L.rijk_sync.argtypes = [_vp]
         L.rijk_fock_energy.argtypes = [_vp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, _dp]
         _LIB = L
     return _LIB
@@ -145,6 +146,9 @@ class FockBuilder:
     def fock_device(self, dD, dMO, n_c, dJ, dK, precision=PREC_FP64):
         """Device-pointer form (ints from tensor.data_ptr()), asynchronous on the context stream."""
         self._check(lib().rijk_fock_device(self._h, _vp(dD), _vp(dMO), int(n_c), _vp(dJ), _vp(dK), precision))
+
+    def sync(self):
+        self._check(lib().rijk_sync(self._h))
 
     def calc_f_ao(self, H, DM, J, K, c=1.0, mc=0, e_nuc=0.0):
         n = self.n
