@@ -258,14 +258,18 @@ def main():
         ms_e2e = float(t.item())
 
     # per-kernel device times (events around each launch on the launching stream)
-    fb.set_profiling(True)
-    stages = {}
-    for _ in range(5):
-        fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), rijk.PREC_FP64)
-        for k, v in fb.stats()["stages"].items():
-            stages.setdefault(k, []).append(v)
-    fb.set_profiling(False)
-    stage_ms = {k: float(np.median(v)) for k, v in stages.items()}
+    def stage_times(prec, reps=5):
+        fb.set_profiling(True)
+        acc = {}
+        for _ in range(reps):
+            fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec)
+            fb.sync()
+            for k, v in fb.stats()["stages"].items():
+                acc.setdefault(k, []).append(v)
+        fb.set_profiling(False)
+        return {k: float(np.median(v)) for k, v in acc.items()}
+
+    stage_ms = stage_times(rijk.PREC_FP64)
     top = max(stage_ms, key=stage_ms.get)
 
     peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
@@ -307,28 +311,55 @@ def main():
     if coul["achieved_gbs"]:
         coul["frac"] = coul["achieved_gbs"] / hbm
 
-    # mixed precision form, if built
+    # mixed precision form (tcgen05 split-BF16 exchange, FP64 Coulomb)
     mixed = None
     try:
         msm = timed(rijk.PREC_MIXED, args.steps, 3)
-        Jm, Km = dJ.cpu().numpy().copy(), dK.cpu().numpy().copy()
+        fb.sync()
+        Km = dK.cpu().numpy().copy()
         fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), rijk.PREC_FP64)
-        torch.cuda.synchronize(dev)
-        mixed = {"value": world * 1e3 / msm, "ms_per_step": msm, "speedup_vs_fp64": ms / msm,
-                 "max_abs_dK_vs_fp64": float(np.max(np.abs(Km - dK.cpu().numpy())))}
+        fb.sync()
+        K64 = dK.cpu().numpy()
+        mstages = stage_times(rijk.PREC_MIXED)
+        mtop = max(mstages, key=mstages.get)
+        mixed = {"value": world * 1e3 / msm, "unit": "builds/s", "ms_per_step": msm, "speedup_vs_fp64": ms / msm,
+                 "max_abs_dK_vs_fp64": float(np.max(np.abs(Km - K64))),
+                 "exchange_energy_err": float(abs(np.sum(DM * (Km - K64)))),
+                 "stage_ms": mstages, "top_kernel": mtop,
+                 "gpu_launches": fb.stats()["kernels_last_fock"] * args.steps}
+        if mtop == "xform_tc":
+            fl = 3 * 2.0 * noccp * (npad2 := ((npad + 127) // 128) * 128) * npad2 * naux
+            mixed["roofline"] = {"kernel": "xform_tc", "bound": "tensor",
+                                 "achieved": fl / (mstages[mtop] * 1e-3) / 1e12, "peak": peaks.get("bf16_tflops", 1590.0),
+                                 "unit": "TFLOP/s", "peak_source": "MEASURED_PEAKS.json bf16_tflops"}
+            mixed["roofline"]["frac"] = mixed["roofline"]["achieved"] / mixed["roofline"]["peak"]
+        elif mtop in ("coulomb_w", "coulomb_j"):
+            bw = tile_elems * naux * 8.0 / (mstages[mtop] * 1e-3) / 1e9
+            mixed["roofline"] = {"kernel": mtop, "bound": "hbm", "achieved": bw, "peak": hbm, "unit": "GB/s",
+                                 "frac": bw / hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
     except rijk.RijkError as e:
         mixed = {"unavailable": str(e)}
 
-    # SCF to convergence with every Fock build on the GPU
+    # SCF to convergence on the GPU (rijk_scf): FP64, and mixed builds switching to FP64
     scf = None
-    if not args.no_scf and rank == 0:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import rijk_oracle as O  # noqa: F401  (only its SCF driver loop is used here)
-        t0 = time.perf_counter()
-        jk = lambda D, C: fb.dm_to_f_transform_ri(D, C, nocc)
-        E, _, _, _, it = O.scf_rhf(si.S, si.H, None, None, nocc, si.Enuc, jk=jk)
-        scf = {"seconds": time.perf_counter() - t0, "iterations": it, "energy": E,
-               "driver": "host DIIS loop, GPU Fock builds (FP64)"}
+    if not args.no_scf:
+        out = {}
+        E64 = None
+        fb.scf(si.H, si.S, nocc, si.Enuc, precision=rijk.PREC_MIXED)  # untimed: first-call set-up
+        for name, prec in (("fp64", rijk.PREC_FP64), ("mixed_then_fp64", rijk.PREC_MIXED)):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            E, _, r = fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, conv_dm_rms=1e-10)
+            el = time.perf_counter() - t0
+            out[name] = {"seconds": el, "iterations": r["iterations"], "iterations_mixed": r["iterations_mixed"],
+                         "energy": E, "ms_fock": r["ms_fock"], "ms_diag": r["ms_diag_phase"],
+                         "converged": bool(r["converged"])}
+            if prec == rijk.PREC_FP64:
+                E64 = E
+            else:
+                out[name]["abs_dE_vs_fp64"] = abs(E - E64)
+        out["criterion"] = "density RMS change < 1e-10; switch to FP64 when max|DIIS error| < 1e-5"
+        scf = out
 
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:

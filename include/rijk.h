@@ -116,6 +116,41 @@ int rijk_sync(rijk_ctx* ctx);
  * The call makes no cudaMalloc, cudaFree or allocating library call. */
 int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ);
 
+/* Options of rijk_scf (zero-initialised fields take the defaults given). */
+typedef struct {
+  int max_iter;           /* default 100                                                        */
+  double conv_dm_rms;     /* converged when RMS(D_new - D) falls below this; default 1e-10     */
+  int precision;          /* RIJK_PREC_FP64, or RIJK_PREC_MIXED: mixed builds until the DIIS
+                             error falls below switch_diis_err, FP64 builds after that        */
+  double switch_diis_err; /* default 1e-5                                                       */
+  int diis_size;          /* default 8                                                          */
+  double lindep;          /* overlap eigenvalues below this are dropped; default 1e-10           */
+} rijk_scf_opts_t;
+
+typedef struct {
+  double energy;          /* E = tr(F D) + tr(H D) + e_nuc of the converged FP64 Fock build     */
+  double dm_rms;          /* last RMS density change                                          */
+  double diis_err;        /* last max |X^T (F D S - S D F) X|                                  */
+  int iterations;         /* Fock builds, the final FP64 one included                          */
+  int iterations_mixed;   /* of which in the mixed form                                        */
+  int converged;
+  int nmo;                /* orbitals kept after removing linear dependence                    */
+  double ms_fock;         /* device time in Fock builds                                        */
+  double ms_total;        /* wall time of rijk_scf                                             */
+  double ms_build_phase;  /* wall time of the Fock-build + DIIS-error phase of the iterations    */
+  double ms_diis_phase;   /* wall time of the Pulay extrapolation phase                         */
+  double ms_diag_phase;   /* wall time of diagonalisation + new density                        */
+} rijk_scf_result_t;
+
+/* Restricted Hartree-Fock on the GPU around the Fock build: the role of the reference's RHF
+ * loop (src/SCF.cpp:78-223), with DIIS on F D S - S D F in place of its SOSCF/L-BFGS step (the
+ * converged energy is the same).  H and S are n x n host arrays; n_c occupied orbitals; the
+ * core-Hamiltonian guess starts it.  Diagonalisation, DIIS extrapolation and the energy are
+ * FP64 on the device.  MO (optional, n x n host) receives the orbitals, one per row, as the
+ * reference's MO_VEC; E as in src/SCF.cpp:134. */
+int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long n_c, double e_nuc, const rijk_scf_opts_t* opts,
+             double* MO, rijk_scf_result_t* result);
+
 /* F = H + (2J - K) c (mc = 0/2) or H + (J - K) 2c (mc = 1), src/molecule.cpp:4418-4430, and
  * E = tr(F D) + tr(H D) + e_nuc (src/SCF.cpp:134); host pointers; F or E may be NULL. */
 int rijk_fock_energy(rijk_ctx* ctx, const double* H, const double* DM, const double* J, const double* K, double c,

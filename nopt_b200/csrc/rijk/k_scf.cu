@@ -1,0 +1,443 @@
+// k_scf.cu — restricted Hartree-Fock on the GPU around the Fock build (rijk_scf).
+//
+// The reference's RHF loop (src/SCF.cpp:78-223) builds D = sum_i C_i C_i^T (src/SCF.cpp:63-73),
+// calls the RI Fock build, forms F = H + 2J - K and E = tr(F D) + tr(H D) + V_nuc
+// (src/SCF.cpp:134) and takes an SOSCF/L-BFGS step.  Here the step is Pulay DIIS on the
+// commutator F D S - S D F in the orthogonal basis X = S^-1/2 (canonical, eigenvalues of S
+// below `lindep` dropped), with diagonalisation of X^T F X; the converged energy is the same.
+// Everything n x n stays on the device in FP64: the small products are cuBLAS DGEMMs, the
+// eigenproblems cuSOLVER syevd, the inner products deterministic two-stage reductions; only
+// the DIIS coefficients ((m+1) x (m+1) system) are solved on the host.
+//
+// Matrices are column-major for cuBLAS.  H, S, F, D, J, K are symmetric, so their row-major
+// and column-major forms coincide; the orbital matrix C (n x nmo, column i = orbital i) has
+// the memory layout of the reference's MO_VEC (row i = orbital i), so its first n_c columns
+// are passed to the Fock build as MO.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dmma.cuh"
+#include "rijk_internal.h"
+
+#define RIJK_API extern "C" __attribute__((visibility("default")))
+
+namespace rijk {
+namespace {
+
+constexpr int kRedBlocks = 256;
+constexpr int kRedThreads = 256;
+constexpr int kOutSlots = 2 + 32 * 33 / 2;  // energy, error, lower triangle of a 32 x 32 Pulay matrix
+
+// partial[b] = sum over a grid-stride slice of f(i)
+template <typename F>
+__global__ void k_reduce_partial(F f, long n, double* __restrict__ partial) {
+  double acc = 0.0;
+  for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<long>(gridDim.x) * blockDim.x)
+    acc += f(i);
+  __shared__ double sh[kRedThreads / 32];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < kRedThreads / 32 ? sh[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  }
+}
+
+template <typename F>
+__global__ void k_reduce_max_partial(F f, long n, double* __restrict__ partial) {
+  double acc = 0.0;
+  for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<long>(gridDim.x) * blockDim.x)
+    acc = fmax(acc, f(i));
+  __shared__ double sh[kRedThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc = fmax(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < kRedThreads / 32 ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  }
+}
+
+// out[slot] = sum (or max) of the kRedBlocks partials, in a fixed order
+__global__ void k_reduce_final(const double* __restrict__ partial, int is_max, double* __restrict__ out, int slot) {
+  double v = (threadIdx.x < kRedBlocks) ? partial[threadIdx.x] : 0.0;
+  __shared__ double sh[kRedBlocks];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = kRedBlocks / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] = is_max ? fmax(sh[threadIdx.x], sh[threadIdx.x + s]) : sh[threadIdx.x] + sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[slot] = sh[0];
+}
+
+struct DotF {
+  const double* a;
+  const double* b;
+  __device__ double operator()(long i) const { return a[i] * b[i]; }
+};
+struct EnergyF {  // D (F + H)
+  const double* d;
+  const double* f;
+  const double* h;
+  __device__ double operator()(long i) const { return d[i] * (f[i] + h[i]); }
+};
+struct DiffSqF {
+  const double* a;
+  const double* b;
+  __device__ double operator()(long i) const {
+    double t = a[i] - b[i];
+    return t * t;
+  }
+};
+struct AbsF {
+  const double* a;
+  __device__ double operator()(long i) const { return fabs(a[i]); }
+};
+
+__global__ void k_scale_cols(const double* __restrict__ U, const double* __restrict__ w, long n, long first,
+                             long nm, double* __restrict__ X) {
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; idx < n * nm; idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    long col = idx / n, row = idx % n;
+    X[idx] = U[row + (first + col) * n] / sqrt(w[first + col]);
+  }
+}
+
+// F = H + 2J - K ; A = F - F^T style antisymmetrisation is done separately
+__global__ void k_fock(const double* __restrict__ H, const double* __restrict__ J, const double* __restrict__ K,
+                       long nn, double* __restrict__ F) {
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; idx < nn; idx += static_cast<long>(gridDim.x) * blockDim.x) F[idx] = H[idx] + 2.0 * J[idx] - K[idx];
+}
+
+// E = A - A^T (column-major n x n)
+__global__ void k_antisym(const double* __restrict__ A, long n, double* __restrict__ E) {
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; idx < n * n; idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    long r = idx % n, c = idx / n;
+    E[idx] = A[idx] - A[c + r * n];
+  }
+}
+
+__global__ void k_axpy_set(double c, const double* __restrict__ x, long n, double* __restrict__ y, int first) {
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; idx < n; idx += static_cast<long>(gridDim.x) * blockDim.x) y[idx] = first ? c * x[idx] : y[idx] + c * x[idx];
+}
+
+unsigned grid_of(long total) {
+  long b = (total + 255) / 256;
+  if (b > 148L * 8) b = 148L * 8;
+  return static_cast<unsigned>(b < 1 ? 1 : b);
+}
+
+// Solves the (m+1) x (m+1) Pulay system by Gaussian elimination with partial pivoting.
+bool diis_coefficients(const std::vector<double>& Bm, int m, std::vector<double>& c) {
+  const int N = m + 1;
+  std::vector<double> A(static_cast<size_t>(N) * N), rhs(N, 0.0);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) A[i * N + j] = Bm[i * m + j];
+  for (int i = 0; i < m; ++i) A[i * N + m] = A[m * N + i] = -1.0;
+  A[m * N + m] = 0.0;
+  rhs[m] = -1.0;
+  for (int k = 0; k < N; ++k) {
+    int p = k;
+    for (int i = k + 1; i < N; ++i)
+      if (std::fabs(A[i * N + k]) > std::fabs(A[p * N + k])) p = i;
+    if (std::fabs(A[p * N + k]) < 1e-300) return false;
+    if (p != k) {
+      for (int j = 0; j < N; ++j) std::swap(A[k * N + j], A[p * N + j]);
+      std::swap(rhs[k], rhs[p]);
+    }
+    for (int i = k + 1; i < N; ++i) {
+      double f = A[i * N + k] / A[k * N + k];
+      for (int j = k; j < N; ++j) A[i * N + j] -= f * A[k * N + j];
+      rhs[i] -= f * rhs[k];
+    }
+  }
+  std::vector<double> x(N);
+  for (int i = N - 1; i >= 0; --i) {
+    double s = rhs[i];
+    for (int j = i + 1; j < N; ++j) s -= A[i * N + j] * x[j];
+    x[i] = s / A[i * N + i];
+  }
+  c.assign(x.begin(), x.begin() + m);
+  for (double v : c)
+    if (!std::isfinite(v)) return false;
+  return true;
+}
+
+}  // namespace
+}  // namespace rijk
+
+using namespace rijk;
+
+RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc, double e_nuc,
+                      const rijk_scf_opts_t* opts, double* MO, rijk_scf_result_t* result) {
+  if (!ctx) return RIJK_ERR_ARG;
+  if (!H || !S || !result) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: null pointer");
+  rijk_scf_opts_t o{};
+  if (opts) o = *opts;
+  if (o.max_iter <= 0) o.max_iter = 100;
+  if (o.conv_dm_rms <= 0) o.conv_dm_rms = 1e-10;
+  if (o.switch_diis_err <= 0) o.switch_diis_err = 1e-5;
+  if (o.diis_size <= 0) o.diis_size = 8;
+  if (o.lindep <= 0) o.lindep = 1e-10;
+  int rc = check_fock_args(ctx, nocc, o.precision);
+  if (rc) return rc;
+  if (o.diis_size > 32) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: diis_size above 32");
+  cudaSetDevice(ctx->device);
+  const auto t_start = std::chrono::steady_clock::now();
+  const long n = ctx->n, nn = n * n;
+  const int ni = static_cast<int>(n);
+  cudaStream_t s = ctx->stream;
+  cublasHandle_t cb = ctx->cublas;
+  cusolverDnHandle_t cs = ctx->cusolver;
+  const int m_max = o.diis_size;
+
+  DeviceBuf dH, dS, dX, dF, dFex, dD, dDn, dC, dJ, dK, dT1, dT2, dE, dW, dU, work, info, red, out, ring_F, ring_E;
+  auto cleanup = [&]() {
+    DeviceBuf* all[] = {&dH, &dS, &dX, &dF, &dFex, &dD, &dDn, &dC, &dJ, &dK, &dT1, &dT2,
+                        &dE, &dW, &dU, &work, &info, &red, &out, &ring_F, &ring_E};
+    for (DeviceBuf* b : all) release(*b);
+  };
+  const size_t b_nn = nn * sizeof(double);
+  if ((rc = ensure(ctx, dH, b_nn, "scf H")) || (rc = ensure(ctx, dS, b_nn, "scf S")) ||
+      (rc = ensure(ctx, dX, b_nn, "scf X")) || (rc = ensure(ctx, dF, b_nn, "scf F")) ||
+      (rc = ensure(ctx, dFex, b_nn, "scf Fex")) || (rc = ensure(ctx, dD, b_nn, "scf D")) ||
+      (rc = ensure(ctx, dDn, b_nn, "scf Dn")) || (rc = ensure(ctx, dC, b_nn, "scf C")) ||
+      (rc = ensure(ctx, dJ, b_nn, "scf J")) || (rc = ensure(ctx, dK, b_nn, "scf K")) ||
+      (rc = ensure(ctx, dT1, b_nn, "scf T1")) || (rc = ensure(ctx, dT2, b_nn, "scf T2")) ||
+      (rc = ensure(ctx, dE, b_nn, "scf E")) || (rc = ensure(ctx, dU, b_nn, "scf U")) ||
+      (rc = ensure(ctx, dW, n * sizeof(double), "scf w")) || (rc = ensure(ctx, info, sizeof(int), "scf info")) ||
+      (rc = ensure(ctx, red, kRedBlocks * sizeof(double), "scf reduce")) ||
+      (rc = ensure(ctx, out, kOutSlots * sizeof(double), "scf out")) ||
+      (rc = ensure(ctx, ring_F, static_cast<size_t>(m_max) * b_nn, "scf DIIS F")) ||
+      (rc = ensure(ctx, ring_E, static_cast<size_t>(m_max) * b_nn, "scf DIIS e"))) {
+    cleanup();
+    return rc;
+  }
+  double* pH = static_cast<double*>(dH.p);
+  double* pS = static_cast<double*>(dS.p);
+  double* pX = static_cast<double*>(dX.p);
+  double* pF = static_cast<double*>(dF.p);
+  double* pFex = static_cast<double*>(dFex.p);
+  double* pD = static_cast<double*>(dD.p);
+  double* pDn = static_cast<double*>(dDn.p);
+  double* pC = static_cast<double*>(dC.p);
+  double* pJ = static_cast<double*>(dJ.p);
+  double* pK = static_cast<double*>(dK.p);
+  double* pT1 = static_cast<double*>(dT1.p);
+  double* pT2 = static_cast<double*>(dT2.p);
+  double* pU = static_cast<double*>(dU.p);
+  double* pW = static_cast<double*>(dW.p);
+  double* pRed = static_cast<double*>(red.p);
+  double* pOut = static_cast<double*>(out.p);
+  double* rF = static_cast<double*>(ring_F.p);
+  double* rE = static_cast<double*>(ring_E.p);
+  int* pInfo = static_cast<int*>(info.p);
+  const double one = 1.0, zero = 0.0;
+
+  auto fail = [&](int code, const char* msg) {
+    cleanup();
+    return set_err(ctx, code, "rijk_scf: %s", msg);
+  };
+  auto reduce = [&](auto f, long count, int is_max, int slot) {
+    if (is_max)
+      k_reduce_max_partial<<<kRedBlocks, kRedThreads, 0, s>>>(f, count, pRed);
+    else
+      k_reduce_partial<<<kRedBlocks, kRedThreads, 0, s>>>(f, count, pRed);
+    k_reduce_final<<<1, kRedBlocks, 0, s>>>(pRed, is_max, pOut, slot);
+  };
+
+  cudaMemcpyAsync(pH, H, b_nn, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(pS, S, b_nn, cudaMemcpyHostToDevice, s);
+
+  // eigensolver workspace: the larger of the S and F' problems (both n x n at most)
+  int lwork = 0;
+  if (cusolverDnDsyevd_bufferSize(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, ni, pU, ni, pW, &lwork) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return fail(RIJK_ERR_SOLVER, "syevd buffer query failed");
+  if ((rc = ensure(ctx, work, static_cast<size_t>(lwork) * sizeof(double), "scf syevd work"))) {
+    cleanup();
+    return rc;
+  }
+  double* pWork = static_cast<double*>(work.p);
+
+  // X = U_k w_k^-1/2 over eigenvalues of S above lindep (ascending: drop the first ndrop)
+  cudaMemcpyAsync(pU, pS, b_nn, cudaMemcpyDeviceToDevice, s);
+  if (cusolverDnDsyevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, ni, pU, ni, pW, pWork, lwork, pInfo) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return fail(RIJK_ERR_SOLVER, "syevd of S failed");
+  std::vector<double> ws(n);
+  int hinfo = 0;
+  cudaMemcpyAsync(ws.data(), pW, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&hinfo, pInfo, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf overlap"))) {
+    cleanup();
+    return rc;
+  }
+  if (hinfo != 0) return fail(RIJK_ERR_SOLVER, "overlap eigendecomposition did not converge");
+  long first = 0;
+  while (first < n && ws[first] < o.lindep) ++first;
+  const long nm = n - first;
+  if (nm < nocc) return fail(RIJK_ERR_ARG, "fewer independent orbitals than n_c");
+  const int nmi = static_cast<int>(nm);
+  k_scale_cols<<<grid_of(n * nm), 256, 0, s>>>(pU, pW, n, first, nm, pX);
+
+  // diagonalise X^T F X -> C = X V (first nm columns of pC)
+  auto diag = [&](const double* Fm) -> int {
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, Fm, ni, pX, ni, &zero, pT1, ni);    // F X
+    cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT1, ni, &zero, pU, nmi);  // X^T F X
+    if (cusolverDnDsyevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nmi, pU, nmi, pW, pWork, lwork,
+                         pInfo) != CUSOLVER_STATUS_SUCCESS)
+      return RIJK_ERR_SOLVER;
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, nmi, &one, pX, ni, pU, nmi, &zero, pC, ni);   // C = X V
+    return RIJK_OK;
+  };
+  auto density = [&](double* Dm) {  // D = C_occ C_occ^T
+    if (nocc > 0)
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, ni, ni, static_cast<int>(nocc), &one, pC, ni, pC, ni, &zero, Dm, ni);
+    else
+      cudaMemsetAsync(Dm, 0, b_nn, s);
+  };
+
+  if (diag(pH) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
+  density(pD);
+
+  int prec = o.precision;
+  int nmix = 0, nbuild = 0, m = 0, head = 0;
+  double ms_fock = 0.0, E = 0.0, err = 1.0, rms = 1.0;
+  bool converged = false;
+  std::vector<double> hout(8);
+  auto build = [&](int p) -> int {
+    int r = fock_device_impl(ctx, pD, pC, nocc, pJ, pK, p);
+    if (r) return r;
+    k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
+    ++nbuild;
+    if (p == RIJK_PREC_MIXED) ++nmix;
+    return RIJK_OK;
+  };
+  double t_build = 0.0, t_diis = 0.0, t_diag = 0.0;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto msec = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+  for (int it = 0; it < o.max_iter; ++it) {
+    auto ta = now();
+    if ((rc = build(prec))) {
+      cleanup();
+      return rc;
+    }
+    // energy and DIIS error X^T (F D S - S D F) X
+    reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pF, ni, pD, ni, &zero, pT1, ni);   // F D
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pT1, ni, pS, ni, &zero, pT2, ni);  // F D S
+    k_antisym<<<grid_of(nn), 256, 0, s>>>(pT2, n, pT1);                                            // FDS - SDF
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, pT1, ni, pX, ni, &zero, pT2, ni);  // e X
+    double* slotE = rE + static_cast<size_t>(head) * nn;
+    double* slotF = rF + static_cast<size_t>(head) * nn;
+    cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT2, ni, &zero, slotE, nmi);  // X^T e X
+    cudaMemcpyAsync(slotF, pF, b_nn, cudaMemcpyDeviceToDevice, s);
+    reduce(AbsF{slotE}, nm * nm, 1, 1);
+    cudaEventRecord(ctx->ev3, s);
+    cudaMemcpyAsync(hout.data(), pOut, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf iteration")) || (rc = check_device_error(ctx))) {
+      cleanup();
+      return rc;
+    }
+    ms_fock += elapsed(ctx->ev0, ctx->ev2);
+    auto tb = now();
+    t_build += msec(ta, tb);
+    E = hout[0] + e_nuc;
+    err = hout[1];
+    if (prec == RIJK_PREC_MIXED && err < o.switch_diis_err) {
+      // switch to the FP64 form: rebuild F for this same density and restart DIIS
+      prec = RIJK_PREC_FP64;
+      m = 0;
+      head = 0;
+      --it;
+      continue;
+    }
+    m = m < m_max ? m + 1 : m_max;
+    head = (head + 1) % m_max;
+    // Pulay B matrix over the stored error vectors
+    std::vector<double> Bm(static_cast<size_t>(m) * m);
+    {
+      int slots[32];
+      for (int i = 0; i < m; ++i) slots[i] = (head - m + i + m_max) % m_max;
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j <= i; ++j)
+          reduce(DotF{rE + static_cast<size_t>(slots[i]) * nn, rE + static_cast<size_t>(slots[j]) * nn}, nm * nm, 0,
+                 2 + i * (i + 1) / 2 + j);
+      std::vector<double> tmp(kOutSlots);
+      cudaMemcpyAsync(tmp.data(), pOut, kOutSlots * sizeof(double), cudaMemcpyDeviceToHost, s);
+      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf DIIS"))) {
+        cleanup();
+        return rc;
+      }
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j <= i; ++j) Bm[i * m + j] = Bm[j * m + i] = tmp[2 + i * (i + 1) / 2 + j];
+      std::vector<double> c;
+      if (!diis_coefficients(Bm, m, c)) {
+        c.assign(m, 0.0);
+        c[m - 1] = 1.0;
+      }
+      for (int i = 0; i < m; ++i)
+        k_axpy_set<<<grid_of(nn), 256, 0, s>>>(c[i], rF + static_cast<size_t>(slots[i]) * nn, nn, pFex, i == 0);
+    }
+    auto tc = now();
+    t_diis += msec(tb, tc);
+    if (diag(pFex) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
+    density(pDn);
+    reduce(DiffSqF{pDn, pD}, nn, 0, 0);
+    cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf density"))) {
+      cleanup();
+      return rc;
+    }
+    rms = std::sqrt(hout[0] / static_cast<double>(nn));
+    t_diag += msec(tc, now());
+    std::swap(pD, pDn);
+    if (rms < o.conv_dm_rms && prec == RIJK_PREC_FP64) {
+      converged = true;
+      break;
+    }
+  }
+  // final FP64 build at the converged density: the energy reported is consistent with D
+  if ((rc = build(RIJK_PREC_FP64))) {
+    cleanup();
+    return rc;
+  }
+  reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
+  cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (MO) cudaMemcpyAsync(MO, pC, static_cast<size_t>(nm) * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf final")) || (rc = check_device_error(ctx))) {
+    cleanup();
+    return rc;
+  }
+  ms_fock += elapsed(ctx->ev0, ctx->ev2);
+  if (MO && nm < n) std::memset(MO + nm * n, 0, static_cast<size_t>(n - nm) * n * sizeof(double));
+  E = hout[0] + e_nuc;
+  result->energy = E;
+  result->dm_rms = rms;
+  result->diis_err = err;
+  result->iterations = nbuild;
+  result->iterations_mixed = nmix;
+  result->converged = converged ? 1 : 0;
+  result->nmo = static_cast<int>(nm);
+  result->ms_fock = ms_fock;
+  result->ms_build_phase = t_build;
+  result->ms_diis_phase = t_diis;
+  result->ms_diag_phase = t_diag;
+  result->ms_total =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  cleanup();
+  if (!converged) return set_err(ctx, RIJK_ERR_CONVERGE, "rijk_scf: not converged in %d iterations", o.max_iter);
+  return RIJK_OK;
+}

@@ -100,7 +100,7 @@ static unsigned grid1d(long total) {
   return static_cast<unsigned>(std::min<long>(std::max<long>(b, 1), 148L * 16));
 }
 
-static float elapsed(cudaEvent_t a, cudaEvent_t b) {
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
     cudaGetLastError();
@@ -132,8 +132,8 @@ static void prof_collect(rijk_ctx* ctx) {
   ctx->stats.profiled_stages = k < 12 ? k : 12;
 }
 
-static int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
-                            int precision) {
+int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
+                     int precision) {
   const long n = ctx->n, naux = ctx->naux, nt = ctx->nt, npad = ctx->npad, ntile = ctx->ntile;
   const long tile_elems = ntile * TILE2;
   cudaStream_t s = ctx->stream;
@@ -477,8 +477,9 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
   return RIJK_OK;
 }
 
+namespace rijk {
 // Reads and clears the device error word the kernels raise instead of trapping.
-static int check_device_error(rijk_ctx* ctx) {
+int check_device_error(rijk_ctx* ctx) {
   int h = 0;
   int rc = cuda_check(ctx, cudaMemcpy(&h, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost), "error word");
   if (rc) return rc;
@@ -488,6 +489,7 @@ static int check_device_error(rijk_ctx* ctx) {
   if (h & DEVERR_NAN) return set_err(ctx, RIJK_ERR_NUMERIC, "non-finite value detected (error bits 0x%x)", h);
   return set_err(ctx, RIJK_ERR_CUDA, "device error bits 0x%x", h);
 }
+}  // namespace rijk
 
 RIJK_API int rijk_sync(rijk_ctx* ctx) {
   if (!ctx) return RIJK_ERR_ARG;
@@ -502,7 +504,8 @@ RIJK_API int rijk_sync(rijk_ctx* ctx) {
   return RIJK_OK;
 }
 
-static int check_fock_args(rijk_ctx* ctx, long nocc, int precision) {
+namespace rijk {
+int check_fock_args(rijk_ctx* ctx, long nocc, int precision) {
   if (!ctx->have_b) return set_err(ctx, RIJK_ERR_STATE, "Fock build before rijk_set_3c");
   if (nocc < 0 || nocc > ctx->n) return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld outside [0, n_ao = %ld]", nocc, ctx->n);
   if (round_up(nocc, 16) > 192) return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld exceeds the supported 192", nocc);
@@ -510,6 +513,7 @@ static int check_fock_args(rijk_ctx* ctx, long nocc, int precision) {
     return set_err(ctx, RIJK_ERR_ARG, "unknown precision %d", precision);
   return RIJK_OK;
 }
+}  // namespace rijk
 
 RIJK_API int rijk_fock_device(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
                               int precision) {

@@ -82,6 +82,18 @@ namespace rijk {
 // Marks the end of one kernel when profiling is on (first call marks the start).
 void prof_mark(rijk_ctx* ctx, const char* name);
 
+// ---- rijk_api.cu
+int set_err(rijk_ctx* ctx, int code, const char* fmt, ...);
+int cuda_check(rijk_ctx* ctx, cudaError_t e, const char* what);
+int ensure(rijk_ctx* ctx, DeviceBuf& b, size_t bytes, const char* what);
+void release(DeviceBuf& b);
+float elapsed(cudaEvent_t a, cudaEvent_t b);
+int check_device_error(rijk_ctx* ctx);
+int check_fock_args(rijk_ctx* ctx, long nocc, int precision);
+// One Fock build on device pointers (J into dJ, K into dK), asynchronous on ctx->stream.
+int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
+                     int precision);
+
 // ---- k_pack.cu
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s);

@@ -39,6 +39,19 @@ class Stats(ctypes.Structure):
                 ("stage_names", (ctypes.c_char * 24) * 12)]
 
 
+class ScfOpts(ctypes.Structure):
+    _fields_ = [("max_iter", ctypes.c_int), ("conv_dm_rms", ctypes.c_double), ("precision", ctypes.c_int),
+                ("switch_diis_err", ctypes.c_double), ("diis_size", ctypes.c_int), ("lindep", ctypes.c_double)]
+
+
+class ScfResult(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("dm_rms", ctypes.c_double), ("diis_err", ctypes.c_double),
+                ("iterations", ctypes.c_int), ("iterations_mixed", ctypes.c_int), ("converged", ctypes.c_int),
+                ("nmo", ctypes.c_int), ("ms_fock", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("ms_build_phase", ctypes.c_double), ("ms_diis_phase", ctypes.c_double),
+                ("ms_diag_phase", ctypes.c_double)]
+
+
 class RijkError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__("rijk error %d: %s" % (code, msg))
@@ -68,6 +81,7 @@ def lib():
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
+        L.rijk_scf.argtypes = [_vp, _dp, _dp, ctypes.c_long, ctypes.c_double, P(ScfOpts), _dp, P(ScfResult)]
         L.rijk_fock_energy.argtypes = [_vp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, _dp]
         _LIB = L
     return _LIB
@@ -146,6 +160,17 @@ class FockBuilder:
     def fock_device(self, dD, dMO, n_c, dJ, dK, precision=PREC_FP64):
         """Device-pointer form (ints from tensor.data_ptr()), asynchronous on the context stream."""
         self._check(lib().rijk_fock_device(self._h, _vp(dD), _vp(dMO), int(n_c), _vp(dJ), _vp(dK), precision))
+
+    def scf(self, H, S, n_c, e_nuc, precision=PREC_FP64, conv_dm_rms=1e-10, switch_diis_err=1e-5, max_iter=100,
+            diis_size=8):
+        """RHF on the GPU (rijk_scf); returns (E, MO rows, result dict)."""
+        n = self.n
+        o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1e-10)
+        r = ScfResult()
+        MO = np.zeros((n, n))
+        self._check(lib().rijk_scf(self._h, _p(_c(H)), _p(_c(S)), int(n_c), float(e_nuc), ctypes.byref(o), _p(MO),
+                                   ctypes.byref(r)))
+        return r.energy, MO, {k: getattr(r, k) for k, _ in ScfResult._fields_}
 
     def sync(self):
         self._check(lib().rijk_sync(self._h))
