@@ -151,6 +151,17 @@ typedef struct {
 int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long n_c, double e_nuc, const rijk_scf_opts_t* opts,
              double* MO, rijk_scf_result_t* result);
 
+/* Adjoint of the Fock build (no reference counterpart; the reference differentiates by finite
+ * differences, src/QM_calc.cpp:142).  For the orbitals MO (n_c rows of n, host) and D = C^T C:
+ *   *E    = tr(F D) + tr(H D) + e_nuc with F = H + 2J - K (FP64 build; src/SCF.cpp:134)
+ *   dEdC  = dE/dMO, n_c x n, = 4 C F (the orbital gradient)
+ *   dEdI3 (optional) = dE/d(P|mu nu) for the packed pairs mu >= nu, laid out as
+ *           RIJK_LAYOUT_PACKED ([pair][P]); a pair mu != nu stands for both (mu nu) and (nu mu)
+ *   dEdPQ (optional) = dE/d(P|Q), naux x naux, entries V_PQ and V_QP taken as independent
+ * Host pointers; synchronous. */
+int rijk_grad(rijk_ctx* ctx, const double* MO, long n_c, const double* H, double e_nuc, double* E, double* dEdC,
+              double* dEdI3, double* dEdPQ);
+
 /* F = H + (2J - K) c (mc = 0/2) or H + (J - K) 2c (mc = 1), src/molecule.cpp:4418-4430, and
  * E = tr(F D) + tr(H D) + e_nuc (src/SCF.cpp:134); host pointers; F or E may be NULL. */
 int rijk_fock_energy(rijk_ctx* ctx, const double* H, const double* DM, const double* J, const double* K, double c,

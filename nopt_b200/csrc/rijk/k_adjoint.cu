@@ -1,0 +1,293 @@
+// k_adjoint.cu — the adjoint of the Fock build (rijk_grad).  No reference counterpart: the
+// reference has no analytic gradient and differentiates by finite differences
+// (src/QM_calc.cpp:142).
+//
+// With D = C^T C over the n_c occupied rows of MO (src/SCF.cpp:63-73), the fitted tensor
+// B^Q = sum_P M_QP (P|.), w_Q = <B^Q, D> and Y^Q = C B^Q C^T (n_c x n_c), the energy of the
+// reference's RHF (src/SCF.cpp:134) is
+//     E = 2 tr(H D) + 2 sum_Q w_Q^2 - sum_Q |Y^Q|^2 + e_nuc ,
+// and its derivatives are
+//     dE/dC        = 4 C F,  F = H + 2J - K                          (orbital gradient)
+//     Gamma^Q      = dE/dB^Q = 4 w_Q D - 2 C^T Y^Q C                 (full-square derivative)
+//     dE/d(P|mu nu) = sum_Q M_QP Gamma^Q_{mu nu}                    (times 2 for mu != nu when the
+//                                                                      pair is stored once)
+//     dE/d(P|Q)    = -(M^T G M)_PQ,  G_QR = (1/2) sum_{mu nu} Gamma^Q_{mu nu} B^R_{mu nu}
+// (E depends on the metric only through V^-1 = M^T M, for either metric form).
+//
+// Device work, FP64 throughout: one FP64 Fock build (which leaves w and the half-transformed
+// XT in the context), then per Q the small products Y^Q = X^Q C^T and T^Q = Y^Q C (cuBLAS
+// strided-batched DGEMM), then k_gamma_f64 forms the packed Gamma tiles
+// Gamma^Q_tile = 4 w_Q D_tile - 2 T^Q_rows T^Q... with DMMA, and two plain DGEMMs contract
+// Gamma with M (raw three-centre gradient) and with B (metric gradient).
+#include <cmath>
+#include <vector>
+
+#include "gemm_f64.cuh"
+#include "rijk_internal.h"
+
+#define RIJK_API extern "C" __attribute__((visibility("default")))
+
+namespace rijk {
+namespace {
+
+constexpr int G_THREADS = 128;
+
+// Gamma[Q][t][r][c] = 4 w_Q D[mu][nu] - 2 sum_i T[Q][mu][i] Ct[nu][i], tile t = (I, J), I >= J.
+// T: [naux][npad][noccp] (row mu, i contiguous); Ct: [npad][noccp]; D: n x n.
+__global__ void __launch_bounds__(G_THREADS)
+    k_gamma_f64(const double* __restrict__ T, const double* __restrict__ Ct, const double* __restrict__ D,
+                const double* __restrict__ w, long n, long npad, long noccp, long tile_elems,
+                double* __restrict__ Gamma) {
+  extern __shared__ __align__(16) double smem_g[];
+  double* sA[2] = {smem_g, smem_g + 64 * LDK};
+  double* sB[2] = {smem_g + 2 * 64 * LDK, smem_g + 3 * 64 * LDK};
+  const long t = blockIdx.x, Q = blockIdx.y;
+  long I, J;
+  tri_decode(t, I, J);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const double* Ar = T + (Q * npad + I * TILE) * noccp;
+  const double* Br = Ct + J * TILE * noccp;
+  auto load = [&](int stage, long k0) {
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+      int idx = tid + it * G_THREADS;
+      int row = idx >> 4, seg = idx & 15;
+      long k = k0 + seg * 2;
+      bool ok = k < noccp;
+      cp_async16(&sA[stage][row * LDK + seg * 2], ok ? Ar + row * noccp + k : T, ok);
+      cp_async16(&sB[stage][row * LDK + seg * 2], ok ? Br + row * noccp + k : Ct, ok);
+    }
+  };
+  double acc[4][4][2];
+  zero_acc(acc);
+  const long nk = (noccp + KC - 1) / KC;
+  load(0, 0);
+  cp_async_commit();
+  for (long kc = 0; kc < nk; ++kc) {
+    if (kc + 1 < nk) {
+      load(static_cast<int>((kc + 1) & 1), (kc + 1) * KC);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    warp_mma_chunk<4, 4, true>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * 32, lane);
+    __syncthreads();
+  }
+  const int g = lane >> 2, tq = lane & 3;
+  const double wq4 = 4.0 * w[Q];
+  double* out = Gamma + Q * tile_elems + t * TILE2;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = wm * 32 + i * 8 + g;
+    const long mu = I * TILE + r;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = wn * 32 + j * 8 + 2 * tq;
+      const long nu = J * TILE + c;
+      double d0 = (mu < n && nu < n) ? D[mu * n + nu] : 0.0;
+      double d1 = (mu < n && nu + 1 < n) ? D[mu * n + nu + 1] : 0.0;
+      *reinterpret_cast<double2*>(out + r * TILE + c) =
+          make_double2(wq4 * d0 - 2.0 * acc[i][j][0], wq4 * d1 - 2.0 * acc[i][j][1]);
+    }
+  }
+}
+
+// Ct[nu][i] = C_{i nu} from the padded MOp[i][nu]
+__global__ void k_transpose_mo(const double* __restrict__ MOp, long noccp, long npad, double* __restrict__ Ct) {
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; idx < noccp * npad; idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    long nu = idx / noccp, i = idx % noccp;
+    Ct[idx] = MOp[i * npad + nu];
+  }
+}
+
+// Scale Gamma in place by the packed-storage weight of its tile (2 off the diagonal, 1 on it).
+__global__ void k_scale_offdiag(double* __restrict__ G, long naux, long ntile, double f_off, double f_diag) {
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long total = naux * ntile * TILE2;
+  for (; idx < total; idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    long t = (idx / TILE2) % ntile;
+    long I, J;
+    tri_decode(t, I, J);
+    G[idx] *= (I == J) ? f_diag : f_off;
+  }
+}
+
+// dI3[(mu(mu+1)/2 + nu) * naux + P] = f(mu, nu) * R[e(mu, nu) + P * te], R column-major (te x naux)
+__global__ void k_gather_pairs(const double* __restrict__ R, long te, long n, long naux, double* __restrict__ out) {
+  const long npair = n * (n + 1) / 2;
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; idx < npair * naux; idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    long pr = idx / naux, P = idx % naux;
+    long mu = static_cast<long>((sqrt(8.0 * static_cast<double>(pr) + 1.0) - 1.0) * 0.5);
+    while (mu * (mu + 1) / 2 > pr) --mu;
+    while ((mu + 1) * (mu + 2) / 2 <= pr) ++mu;
+    long nu = pr - mu * (mu + 1) / 2;
+    long I = mu / TILE, J = nu / TILE;
+    long e = tri_index(I, J) * TILE2 + (mu % TILE) * TILE + (nu % TILE);
+    out[idx] = (mu == nu ? 1.0 : 2.0) * R[e + P * te];
+  }
+}
+
+__global__ void k_fock_sym(const double* __restrict__ H, const double* __restrict__ J, const double* __restrict__ K,
+                           long nn, double* __restrict__ F) {
+  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; idx < nn; idx += static_cast<long>(gridDim.x) * blockDim.x) F[idx] = H[idx] + 2.0 * J[idx] - K[idx];
+}
+
+__global__ void k_energy_partial(const double* __restrict__ D, const double* __restrict__ F,
+                                 const double* __restrict__ H, long nn, double* __restrict__ partial) {
+  double acc = 0.0;
+  for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < nn; i += static_cast<long>(gridDim.x) * blockDim.x)
+    acc += D[i] * (F[i] + H[i]);
+  acc = warp_sum(acc);
+  __shared__ double sh[8];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < 8; ++i) s += sh[i];
+    partial[blockIdx.x] = s;
+  }
+}
+
+unsigned grid_of(long total) {
+  long b = (total + 255) / 256;
+  if (b > 148L * 16) b = 148L * 16;
+  return static_cast<unsigned>(b < 1 ? 1 : b);
+}
+
+}  // namespace
+}  // namespace rijk
+
+using namespace rijk;
+
+RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double* H, double e_nuc, double* E,
+                       double* dEdC, double* dEdI3, double* dEdPQ) {
+  if (!ctx) return RIJK_ERR_ARG;
+  if (!MO || !H || !E || !dEdC) return set_err(ctx, RIJK_ERR_ARG, "rijk_grad: null pointer");
+  int rc = check_fock_args(ctx, nocc, RIJK_PREC_FP64);
+  if (rc) return rc;
+  if (nocc < 1) return set_err(ctx, RIJK_ERR_ARG, "rijk_grad: n_c must be at least 1");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  cublasHandle_t cb = ctx->cublas;
+  const long n = ctx->n, naux = ctx->naux, npad = ctx->npad, nt = ctx->nt, ntile = ctx->ntile;
+  const long nn = n * n, te = ntile * TILE2, noccp = round_up(nocc, 16), nauxp = round_up(naux, KC);
+  const int ni = static_cast<int>(n), nci = static_cast<int>(nocc);
+  const double one = 1.0, zero = 0.0;
+  const size_t b_nn = nn * sizeof(double);
+  DeviceBuf dMO, dH, dD, dJ, dK, dF, dG, red, Y, Tb, Ct, Gam, R, Gm, T1, out;
+  auto cleanup = [&]() {
+    DeviceBuf* all[] = {&dMO, &dH, &dD, &dJ, &dK, &dF, &dG, &red, &Y, &Tb, &Ct, &Gam, &R, &Gm, &T1, &out};
+    for (DeviceBuf* b : all) release(*b);
+  };
+  auto chk = [&](int r) {
+    if (r) cleanup();
+    return r;
+  };
+  if ((rc = chk(ensure(ctx, dMO, nocc * n * sizeof(double), "grad MO"))) || (rc = chk(ensure(ctx, dH, b_nn, "grad H"))) ||
+      (rc = chk(ensure(ctx, dD, b_nn, "grad D"))) || (rc = chk(ensure(ctx, dJ, b_nn, "grad J"))) ||
+      (rc = chk(ensure(ctx, dK, b_nn, "grad K"))) || (rc = chk(ensure(ctx, dF, b_nn, "grad F"))) ||
+      (rc = chk(ensure(ctx, dG, nocc * n * sizeof(double), "grad dEdC"))) ||
+      (rc = chk(ensure(ctx, red, 512 * sizeof(double), "grad reduce"))))
+    return rc;
+  double* pMO = static_cast<double*>(dMO.p);
+  double* pD = static_cast<double*>(dD.p);
+  double* pF = static_cast<double*>(dF.p);
+  cudaMemcpyAsync(pMO, MO, nocc * n * sizeof(double), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dH.p, H, b_nn, cudaMemcpyHostToDevice, s);
+  // D = C^T C: MO row-major (n_c x n) is column-major (n x n_c)
+  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, ni, ni, nci, &one, pMO, ni, pMO, ni, &zero, pD, ni);
+  if ((rc = chk(fock_device_impl(ctx, pD, pMO, nocc, static_cast<double*>(dJ.p), static_cast<double*>(dK.p),
+                                 RIJK_PREC_FP64))))
+    return rc;
+  k_fock_sym<<<grid_of(nn), 256, 0, s>>>(static_cast<const double*>(dH.p), static_cast<const double*>(dJ.p),
+                                         static_cast<const double*>(dK.p), nn, pF);
+  k_energy_partial<<<512, 256, 0, s>>>(pD, pF, static_cast<const double*>(dH.p), nn, static_cast<double*>(red.p));
+  // dE/dC = 4 C F  (column-major n x n_c = 4 F Mt)
+  const double four = 4.0;
+  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nci, ni, &four, pF, ni, pMO, ni, &zero, static_cast<double*>(dG.p), ni);
+  std::vector<double> part(512);
+  cudaMemcpyAsync(part.data(), red.p, 512 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(dEdC, dG.p, nocc * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if ((rc = chk(cuda_check(ctx, cudaStreamSynchronize(s), "rijk_grad energy"))) || (rc = chk(check_device_error(ctx))))
+    return rc;
+  double e = e_nuc;
+  for (double v : part) e += v;
+  *E = e;
+  if (!dEdI3 && !dEdPQ) {
+    cleanup();
+    return RIJK_OK;
+  }
+  // per-Q small products over the half-transformed tensor XT[nu][Q*noccp + i] of the FP64 build
+  const long kdim = naux * noccp;
+  if ((rc = chk(ensure(ctx, Y, static_cast<size_t>(naux) * noccp * noccp * sizeof(double), "grad Y"))) ||
+      (rc = chk(ensure(ctx, Tb, static_cast<size_t>(naux) * npad * noccp * sizeof(double), "grad T"))) ||
+      (rc = chk(ensure(ctx, Ct, static_cast<size_t>(npad) * noccp * sizeof(double), "grad Ct"))) ||
+      (rc = chk(ensure(ctx, Gam, static_cast<size_t>(naux) * te * sizeof(double), "grad Gamma"))))
+    return rc;
+  const double* XT = static_cast<const double*>(ctx->XT.p);
+  const double* MOp = static_cast<const double*>(ctx->MOp.p);
+  const int ncp = static_cast<int>(noccp), npi = static_cast<int>(npad);
+  // Y^Q (noccp x noccp) = X^Q (noccp x npad, column-major view of XT, ld kdim) . Cm (npad x noccp)
+  cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, ncp, ncp, npi, &one, XT, static_cast<int>(kdim), noccp, MOp,
+                            npi, 0, &zero, static_cast<double*>(Y.p), ncp, noccp * noccp, static_cast<int>(naux));
+  // T^Q as [mu][i] = (Y^Q C) column-major (noccp x npad): Y^Q (noccp x noccp) . Cm^T
+  cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_T, ncp, npi, ncp, &one, static_cast<const double*>(Y.p), ncp,
+                            noccp * noccp, MOp, npi, 0, &zero, static_cast<double*>(Tb.p), ncp, npad * noccp,
+                            static_cast<int>(naux));
+  k_transpose_mo<<<grid_of(noccp * npad), 256, 0, s>>>(MOp, noccp, npad, static_cast<double*>(Ct.p));
+  {
+    const size_t smem = 4 * 64 * LDK * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_gamma_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      attr = true;
+    }
+    dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(naux));
+    k_gamma_f64<<<grid, G_THREADS, smem, s>>>(static_cast<const double*>(Tb.p), static_cast<const double*>(Ct.p), pD,
+                                              static_cast<const double*>(ctx->w.p), n, npad, noccp, te,
+                                              static_cast<double*>(Gam.p));
+  }
+  release(Y);
+  release(Tb);
+  double* pGam = static_cast<double*>(Gam.p);
+  const double* pM = static_cast<const double*>(ctx->M.p);  // row-major [Q][P], ld nauxp
+  const int na = static_cast<int>(naux), nap = static_cast<int>(nauxp), tei = static_cast<int>(te);
+  if (dEdI3) {
+    // R (te x naux, column-major) = Gamma_cm (te x naux) . M_cm^T, M_cm(P, Q) = M[Q][P]
+    if ((rc = chk(ensure(ctx, R, static_cast<size_t>(te) * naux * sizeof(double), "grad R"))) ||
+        (rc = chk(ensure(ctx, out, static_cast<size_t>(n * (n + 1) / 2) * naux * sizeof(double), "grad dI3"))))
+      return rc;
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, tei, na, na, &one, pGam, tei, pM, nap, &zero, static_cast<double*>(R.p),
+                tei);
+    k_gather_pairs<<<grid_of(n * (n + 1) / 2 * naux), 256, 0, s>>>(static_cast<const double*>(R.p), te, n, naux,
+                                                                   static_cast<double*>(out.p));
+    cudaMemcpyAsync(dEdI3, out.p, static_cast<size_t>(n * (n + 1) / 2) * naux * sizeof(double),
+                    cudaMemcpyDeviceToHost, s);
+  }
+  if (dEdPQ) {
+    // G = 1/2 sum_e omega_e Gamma[Q][e] B[R][e] (omega = 2 off-diagonal tiles); dE/dV = -M^T G M
+    if ((rc = chk(ensure(ctx, Gm, static_cast<size_t>(naux) * naux * sizeof(double), "grad G"))) ||
+        (rc = chk(ensure(ctx, T1, static_cast<size_t>(naux) * naux * sizeof(double), "grad T1"))))
+      return rc;
+    k_scale_offdiag<<<grid_of(naux * te), 256, 0, s>>>(pGam, naux, ntile, 2.0, 1.0);
+    const double half = 0.5, mone = -1.0;
+    cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, na, na, tei, &half, pGam, tei, static_cast<const double*>(ctx->B.p), tei,
+                &zero, static_cast<double*>(Gm.p), na);
+    // T1 = G M_cm^T ; dEdPQ = -M_cm T1   (M_cm = M^T as a column-major naux x naux block, ld nauxp)
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, na, na, na, &one, static_cast<const double*>(Gm.p), na, pM, nap, &zero,
+                static_cast<double*>(T1.p), na);
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, na, na, na, &mone, pM, nap, static_cast<const double*>(T1.p), na, &zero,
+                static_cast<double*>(Gm.p), na);
+    cudaMemcpyAsync(dEdPQ, Gm.p, static_cast<size_t>(naux) * naux * sizeof(double), cudaMemcpyDeviceToHost, s);
+  }
+  rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_grad");
+  cleanup();
+  (void)nt;
+  return rc;
+}

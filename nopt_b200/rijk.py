@@ -81,6 +81,7 @@ def lib():
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
+        L.rijk_grad.argtypes = [_vp, _dp, ctypes.c_long, _dp, ctypes.c_double, _dp, _dp, _dp, _dp]
         L.rijk_scf.argtypes = [_vp, _dp, _dp, ctypes.c_long, ctypes.c_double, P(ScfOpts), _dp, P(ScfResult)]
         L.rijk_fock_energy.argtypes = [_vp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, _dp]
         _LIB = L
@@ -171,6 +172,18 @@ class FockBuilder:
         self._check(lib().rijk_scf(self._h, _p(_c(H)), _p(_c(S)), int(n_c), float(e_nuc), ctypes.byref(o), _p(MO),
                                    ctypes.byref(r)))
         return r.energy, MO, {k: getattr(r, k) for k, _ in ScfResult._fields_}
+
+    def grad(self, MO, n_c, H, e_nuc, want_3c=False, want_metric=False):
+        """(E, dE/dMO (n_c x n), dE/d(P|mu nu) packed [pair][P] or None, dE/d(P|Q) or None)."""
+        n = self.n
+        MO = _c(MO[:n_c])
+        E = ctypes.c_double(0.0)
+        dC = np.empty((n_c, n))
+        d3 = np.empty((n * (n + 1) // 2, self.naux)) if want_3c else None
+        dV = np.empty((self.naux, self.naux)) if want_metric else None
+        self._check(lib().rijk_grad(self._h, _p(MO), int(n_c), _p(_c(H)), float(e_nuc), ctypes.byref(E), _p(dC),
+                                    _p(d3), _p(dV)))
+        return E.value, dC, d3, dV
 
     def sync(self):
         self._check(lib().rijk_sync(self._h))

@@ -133,6 +133,47 @@ def jk_from_b(Bp, n, DM, MO, n_c):
     return J, K
 
 
+# ----------------------------------------------------------------- adjoint ------
+def energy_from_mo(RI_AA, Vm05, H, MO, n_c, Enuc):
+    """E(C) of the reference's RHF (src/SCF.cpp:134) with D = C^T C from the first n_c rows."""
+    n = H.shape[0]
+    DM = gen_hf_dm(MO, n, n_c)
+    J, K = dm_to_f_transform_ri(RI_AA, Vm05, DM, MO, n_c, n)
+    F = calc_f_ao(H, J, K)
+    return rhf_energy(F, H, DM, Enuc), F
+
+
+def adjoint_reference(I3_packed, M, H, MO, n_c, Enuc):
+    """E and its derivatives from the closed forms, for a metric factor M with M^T M = V^-1:
+    E = 2 tr(HD) + 2 sum_Q w_Q^2 - sum_Q |Y^Q|^2 + Enuc, w_Q = <B^Q, D>, Y^Q = C B^Q C^T;
+    dE/dC = 4 C F; Gamma^Q = 4 w_Q D - 2 C^T Y^Q C; dE/d(P|mu nu) = sum_Q M_QP Gamma^Q
+    (x2 for a packed off-diagonal pair); dE/d(P|Q) = -M^T G M, G = 1/2 <Gamma^Q, B^R>."""
+    n = H.shape[0]
+    naux = M.shape[0]
+    Bf = np.zeros((naux, n, n))
+    Bp = M @ I3_packed.T
+    il = np.tril_indices(n)
+    Bf[:, il[0], il[1]] = Bp
+    Bf[:, il[1], il[0]] = Bp
+    C = MO[:n_c]
+    D = C.T @ C
+    w = np.einsum("qmn,mn->q", Bf, D)
+    X = np.einsum("im,qmn->qin", C, Bf)
+    Y = np.einsum("qin,jn->qij", X, C)
+    J = np.einsum("q,qmn->mn", w, Bf)
+    K = np.einsum("qim,qin->mn", X, X)
+    F = H + 2 * J - K
+    E = 2 * np.sum(H * D) + 2 * np.sum(w * w) - np.sum(Y * Y) + Enuc
+    dC = 4 * C @ F
+    Gam = 4 * w[:, None, None] * D[None] - 2 * np.einsum("im,qij,jn->qmn", C, Y, C)
+    d3f = np.einsum("qp,qmn->pmn", M, Gam)
+    fac = np.where(il[0] == il[1], 1.0, 2.0)
+    d3 = (d3f[:, il[0], il[1]] * fac).T.copy()
+    G = 0.5 * np.einsum("qmn,rmn->qr", Gam, Bf)
+    dV = -M.T @ G @ M
+    return E, dC, d3, dV
+
+
 # --------------------------------------------------------------------- SCF ------
 def scf_rhf(S, H, RI_AA, Vm05, n_occ, Enuc, conv_dm=1e-10, max_iter=100, diis_n=8, jk=None):
     """Restricted HF with DIIS on F D S - S D F, using the reference's J/K, F and E
