@@ -56,6 +56,15 @@ int gto_coulomb_2c(const gto_basis* aux, double* V);
 /* Three-centre Coulomb integrals (mu nu|P) in one of the GTO_3C_* layouts. */
 int gto_coulomb_3c(const gto_basis* orb, const gto_basis* aux, int layout, double* out);
 
+/* Density of one atom (nuclear charge Z at xyz) for a superposition-of-atomic-densities start:
+ * spherically averaged RHF with fractional occupations in the atom's orbital basis `orb`,
+ * RI-JK in its fitting basis `aux`.  D (n x n) uses the reference's normalisation (trace of
+ * D S = Z / 2); rows (at most n x n) receive nrows factor rows sqrt(f_k) v_k with
+ * D = sum_k rows_k^T rows_k, usable as MO rows of a Fock build (the reference's SAD start,
+ * src/sad_guess.cpp:165-215). */
+int gto_atomic_density(const gto_basis* orb, const gto_basis* aux, double Z, const double* xyz, double* D,
+                       double* rows, int* nrows);
+
 /* Boys function F_m(T), m = 0..mmax (test hook). */
 int gto_boys(int mmax, double T, double* F);
 

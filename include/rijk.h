@@ -122,9 +122,16 @@ typedef struct {
   double conv_dm_rms;     /* converged when RMS(D_new - D) falls below this; default 1e-10     */
   int precision;          /* RIJK_PREC_FP64, or RIJK_PREC_MIXED: mixed builds until the DIIS
                              error falls below switch_diis_err, FP64 builds after that        */
-  double switch_diis_err; /* default 1e-5                                                       */
+  double switch_diis_err; /* default 1e-5; the switch also happens when the mixed-phase error has
+                             not improved for 5 iterations or after max_iter / 2 mixed iterations */
   int diis_size;          /* default 8                                                          */
   double lindep;          /* overlap eigenvalues below this are dropped; default 1e-10           */
+  /* Optional start (host arrays): a density D0 (n x n) with factor rows R (guess_nrows x n),
+   * D0 = R^T R, e.g. a superposition of atomic densities; its FP64 Fock build replaces the
+   * core-Hamiltonian start (the reference's SAD start, src/sad_guess.cpp:199-201). */
+  const double* guess_dm;
+  const double* guess_rows;
+  long guess_nrows;
 } rijk_scf_opts_t;
 
 typedef struct {
@@ -140,6 +147,10 @@ typedef struct {
   double ms_build_phase;  /* wall time of the Fock-build + DIIS-error phase of the iterations    */
   double ms_diis_phase;   /* wall time of the Pulay extrapolation phase                         */
   double ms_diag_phase;   /* wall time of diagonalisation + new density                        */
+  int history_len;        /* entries of the per-iteration trace below (first 128 iterations)   */
+  double history_energy[128];
+  double history_diis_err[128];
+  int history_mixed[128]; /* 1 where the iteration used the mixed form                          */
 } rijk_scf_result_t;
 
 /* Restricted Hartree-Fock on the GPU around the Fock build: the role of the reference's RHF

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-HOST_SOURCES = ["host/gto_ints.cpp"]
+HOST_SOURCES = ["host/gto_ints.cpp", "host/gto_guess.cpp"]
 CUDA_SOURCES = [
     "rijk/rijk_api.cu",
     "rijk/k_pack.cu",

@@ -20,7 +20,7 @@ constexpr int X_THREADS = 128;
 template <int NF>
 __global__ void __launch_bounds__(X_THREADS)
     k_xform_f64(const double* __restrict__ B, const double* __restrict__ MOp, long nt, long npad, long tile_elems,
-                long kdim, double* __restrict__ XT) {
+                long kdim, long noccp_total, long i0, double* __restrict__ XT) {
   constexpr int NOCCP = NF * 16;
   constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
   constexpr int B_STAGE = NOCCP * LDK;
@@ -86,15 +86,17 @@ __global__ void __launch_bounds__(X_THREADS)
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     long nu = J * TILE + wm * 32 + i * 8 + g;
-    double* row = XT + nu * kdim + Q * NOCCP + wn * (NOCCP / 2);
+    double* row = XT + nu * kdim + Q * noccp_total + i0 + wn * (NOCCP / 2);
 #pragma unroll
     for (int j = 0; j < NF; ++j)
       *reinterpret_cast<double2*>(row + j * 8 + 2 * tq) = make_double2(acc[i][j][0], acc[i][j][1]);
   }
 }
 
+// One orbital batch: rows i0 .. i0 + NF*16 of MOp into columns Q*noccp_total + i0 + ... of XT.
 template <int NF>
-static void launch_xform_nf(const double* B, const double* MOp, long naux, long nt, double* XT, cudaStream_t s) {
+static void launch_xform_nf(const double* B, const double* MOp, long naux, long nt, long noccp_total, long i0,
+                            double* XT, cudaStream_t s) {
   constexpr int NOCCP = NF * 16;
   constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
   size_t smem = (2 * A_STAGE + 2 * NOCCP * LDK) * sizeof(double);
@@ -106,24 +108,25 @@ static void launch_xform_nf(const double* B, const double* MOp, long naux, long 
   long npad = nt * TILE;
   long tile_elems = nt * (nt + 1) / 2 * TILE2;
   dim3 grid(static_cast<unsigned>(nt), static_cast<unsigned>(naux));
-  k_xform_f64<NF><<<grid, X_THREADS, smem, s>>>(B, MOp, nt, npad, tile_elems, naux * NOCCP, XT);
+  k_xform_f64<NF><<<grid, X_THREADS, smem, s>>>(B, MOp + i0 * npad, nt, npad, tile_elems, naux * noccp_total,
+                                                 noccp_total, i0, XT);
 }
 
+// The orbitals go in batches of at most 96 (NF <= 6 keeps the accumulators in registers).
 void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s) {
-  switch (noccp / 16) {
-    case 1: launch_xform_nf<1>(B, MOp, naux, nt, XT, s); break;
-    case 2: launch_xform_nf<2>(B, MOp, naux, nt, XT, s); break;
-    case 3: launch_xform_nf<3>(B, MOp, naux, nt, XT, s); break;
-    case 4: launch_xform_nf<4>(B, MOp, naux, nt, XT, s); break;
-    case 5: launch_xform_nf<5>(B, MOp, naux, nt, XT, s); break;
-    case 6: launch_xform_nf<6>(B, MOp, naux, nt, XT, s); break;
-    case 7: launch_xform_nf<7>(B, MOp, naux, nt, XT, s); break;
-    case 8: launch_xform_nf<8>(B, MOp, naux, nt, XT, s); break;
-    case 9: launch_xform_nf<9>(B, MOp, naux, nt, XT, s); break;
-    case 10: launch_xform_nf<10>(B, MOp, naux, nt, XT, s); break;
-    case 11: launch_xform_nf<11>(B, MOp, naux, nt, XT, s); break;
-    case 12: launch_xform_nf<12>(B, MOp, naux, nt, XT, s); break;
-    default: break;  // rejected by the API (n_c > 192)
+  const long nb = (noccp + 95) / 96;
+  const long per = round_up((noccp + nb - 1) / nb, 16);
+  for (long i0 = 0; i0 < noccp; i0 += per) {
+    const long cnt = (noccp - i0 < per) ? noccp - i0 : per;
+    switch (cnt / 16) {
+      case 1: launch_xform_nf<1>(B, MOp, naux, nt, noccp, i0, XT, s); break;
+      case 2: launch_xform_nf<2>(B, MOp, naux, nt, noccp, i0, XT, s); break;
+      case 3: launch_xform_nf<3>(B, MOp, naux, nt, noccp, i0, XT, s); break;
+      case 4: launch_xform_nf<4>(B, MOp, naux, nt, noccp, i0, XT, s); break;
+      case 5: launch_xform_nf<5>(B, MOp, naux, nt, noccp, i0, XT, s); break;
+      case 6: launch_xform_nf<6>(B, MOp, naux, nt, noccp, i0, XT, s); break;
+      default: break;
+    }
   }
 }
 

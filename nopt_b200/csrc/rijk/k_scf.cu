@@ -193,6 +193,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   int rc = check_fock_args(ctx, nocc, o.precision);
   if (rc) return rc;
   if (o.diis_size > 32) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: diis_size above 32");
+  if (o.guess_dm && (!o.guess_rows || o.guess_nrows <= 0 || o.guess_nrows > round_up(ctx->n, 16)))
+    return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: guess needs factor rows (1 .. n_ao of them)");
   cudaSetDevice(ctx->device);
   const auto t_start = std::chrono::steady_clock::now();
   const long n = ctx->n, nn = n * n;
@@ -309,12 +311,38 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       cudaMemsetAsync(Dm, 0, b_nn, s);
   };
 
-  if (diag(pH) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
+  if (o.guess_dm && o.guess_rows && o.guess_nrows > 0) {
+    // start from the given density: one FP64 build with its factor rows, then diagonalise
+    DeviceBuf dR;
+    if ((rc = ensure(ctx, dR, static_cast<size_t>(o.guess_nrows) * n * sizeof(double), "scf guess rows"))) {
+      cleanup();
+      return rc;
+    }
+    cudaMemcpyAsync(pD, o.guess_dm, b_nn, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dR.p, o.guess_rows, static_cast<size_t>(o.guess_nrows) * n * sizeof(double),
+                    cudaMemcpyHostToDevice, s);
+    rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, RIJK_PREC_FP64);
+    if (!rc) {
+      k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
+      rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf guess");
+    }
+    release(dR);
+    if (rc) {
+      cleanup();
+      return rc;
+    }
+    if (diag(pF) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the guess Fock matrix failed");
+  } else {
+    if (diag(pH) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
+  }
   density(pD);
 
   int prec = o.precision;
   int nmix = 0, nbuild = 0, m = 0, head = 0;
   double ms_fock = 0.0, E = 0.0, err = 1.0, rms = 1.0;
+  double best_err = 1e300;
+  int since_best = 0;
+  result->history_len = 0;
   bool converged = false;
   std::vector<double> hout(8);
   auto build = [&](int p) -> int {
@@ -356,7 +384,24 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     t_build += msec(ta, tb);
     E = hout[0] + e_nuc;
     err = hout[1];
-    if (prec == RIJK_PREC_MIXED && err < o.switch_diis_err) {
+    if (result->history_len < 128) {
+      result->history_energy[result->history_len] = E;
+      result->history_diis_err[result->history_len] = err;
+      result->history_mixed[result->history_len] = prec == RIJK_PREC_MIXED ? 1 : 0;
+      ++result->history_len;
+    }
+    bool stalled = false;
+    if (prec == RIJK_PREC_MIXED) {
+      if (err < best_err * 0.9) {
+        best_err = err;
+        since_best = 0;
+      } else {
+        ++since_best;
+      }
+      // the split-BF16 rounding noise can put a floor under the DIIS error: stop waiting for it
+      stalled = since_best >= 5 || nmix >= o.max_iter / 2;
+    }
+    if (prec == RIJK_PREC_MIXED && (err < o.switch_diis_err || stalled)) {
       // switch to the FP64 form: rebuild F for this same density and restart DIIS
       prec = RIJK_PREC_FP64;
       m = 0;

@@ -507,10 +507,14 @@ RIJK_API int rijk_sync(rijk_ctx* ctx) {
 namespace rijk {
 int check_fock_args(rijk_ctx* ctx, long nocc, int precision) {
   if (!ctx->have_b) return set_err(ctx, RIJK_ERR_STATE, "Fock build before rijk_set_3c");
-  if (nocc < 0 || nocc > ctx->n) return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld outside [0, n_ao = %ld]", nocc, ctx->n);
-  if (round_up(nocc, 16) > 192) return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld exceeds the supported 192", nocc);
+  if (nocc < 0 || nocc > round_up(ctx->n, 16))
+    return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld outside [0, n_ao = %ld]", nocc, ctx->n);
   if (precision != RIJK_PREC_FP64 && precision != RIJK_PREC_MIXED)
     return set_err(ctx, RIJK_ERR_ARG, "unknown precision %d", precision);
+  // the FP64 half-transform runs in orbital batches (any n_c); the tcgen05 form holds all n_c
+  // columns of one aux function in TMEM (N <= 192)
+  if (precision == RIJK_PREC_MIXED && round_up(nocc, 16) > 192)
+    return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld exceeds the 192 of the mixed form", nocc);
   return RIJK_OK;
 }
 }  // namespace rijk

@@ -11,6 +11,7 @@ import os
 import numpy as np
 
 from . import basis as _basis
+from .molecules import Molecule
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -42,6 +43,7 @@ def lib():
         L.gto_coulomb_2c.argtypes = [ctypes.c_void_p, _dp]
         L.gto_coulomb_3c.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _dp]
         L.gto_boys.argtypes = [ctypes.c_int, ctypes.c_double, _dp]
+        L.gto_atomic_density.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, _dp, _dp, _dp, _ip]
         L.gto_set_threads.argtypes = [ctypes.c_int]
         L.gto_set_threads.restype = None
         _LIB = L
@@ -132,6 +134,44 @@ def coulomb_3c(orb, aux, layout=LAYOUT_PACKED):
     return out
 
 
+def atomic_density(sym, orb_basis, aux_basis):
+    """(D, rows) of one atom of element `sym` at the origin (see gto_atomic_density)."""
+    from .molecules import Z_OF
+    at = Molecule([sym], [[0.0, 0.0, 0.0]])
+    orb = Basis.for_molecule(orb_basis, at)
+    aux = Basis.for_molecule(aux_basis, at)
+    n = orb.nbf
+    D = np.empty((n, n))
+    rows = np.empty((n, n))
+    nr = ctypes.c_int(0)
+    xyz = np.zeros(3)
+    _check(lib().gto_atomic_density(orb._h, aux._h, float(Z_OF[sym]), _ptr(xyz), _ptr(D), _ptr(rows),
+                                    ctypes.byref(nr)), "gto_atomic_density")
+    return D, rows[:nr.value].copy()
+
+
+def sad_guess(mol, orb_basis, aux_basis):
+    """Block-diagonal superposition of atomic densities over the molecule's atoms (in basis order)
+    and its factor rows, D0 = R^T R, the reference's SAD start (src/sad_guess.cpp:165-215)."""
+    cache = {}
+    blocks = []
+    for sym in mol.symbols:
+        if sym not in cache:
+            cache[sym] = atomic_density(sym, orb_basis, aux_basis)
+        blocks.append(cache[sym])
+    n = sum(b[0].shape[0] for b in blocks)
+    D = np.zeros((n, n))
+    R = np.zeros((sum(b[1].shape[0] for b in blocks), n))
+    o = r = 0
+    for Da, Ra in blocks:
+        na, nr = Da.shape[0], Ra.shape[0]
+        D[o:o + na, o:o + na] = Da
+        R[r:r + nr, o:o + na] = Ra
+        o += na
+        r += nr
+    return D, R
+
+
 def boys(mmax, T):
     F = np.empty(mmax + 1)
     _check(lib().gto_boys(mmax, T, _ptr(F)), "gto_boys")
@@ -156,6 +196,11 @@ class SystemIntegrals:
         self.I3 = coulomb_3c(self.orb, self.aux, layout)
         self.Enuc = mol.nuclear_repulsion()
         self.nocc = mol.nelec // 2
+        self.orb_name, self.aux_name = orb_basis, aux_basis
+
+    def sad(self):
+        """(D0, factor rows) of the superposition-of-atomic-densities start."""
+        return sad_guess(self.mol, self.orb_name, self.aux_name)
 
     @property
     def n(self):

@@ -41,7 +41,8 @@ class Stats(ctypes.Structure):
 
 class ScfOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv_dm_rms", ctypes.c_double), ("precision", ctypes.c_int),
-                ("switch_diis_err", ctypes.c_double), ("diis_size", ctypes.c_int), ("lindep", ctypes.c_double)]
+                ("switch_diis_err", ctypes.c_double), ("diis_size", ctypes.c_int), ("lindep", ctypes.c_double),
+                ("guess_dm", _dp), ("guess_rows", _dp), ("guess_nrows", ctypes.c_long)]
 
 
 class ScfResult(ctypes.Structure):
@@ -49,7 +50,9 @@ class ScfResult(ctypes.Structure):
                 ("iterations", ctypes.c_int), ("iterations_mixed", ctypes.c_int), ("converged", ctypes.c_int),
                 ("nmo", ctypes.c_int), ("ms_fock", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("ms_build_phase", ctypes.c_double), ("ms_diis_phase", ctypes.c_double),
-                ("ms_diag_phase", ctypes.c_double)]
+                ("ms_diag_phase", ctypes.c_double), ("history_len", ctypes.c_int),
+                ("history_energy", ctypes.c_double * 128), ("history_diis_err", ctypes.c_double * 128),
+                ("history_mixed", ctypes.c_int * 128)]
 
 
 class RijkError(RuntimeError):
@@ -163,15 +166,24 @@ class FockBuilder:
         self._check(lib().rijk_fock_device(self._h, _vp(dD), _vp(dMO), int(n_c), _vp(dJ), _vp(dK), precision))
 
     def scf(self, H, S, n_c, e_nuc, precision=PREC_FP64, conv_dm_rms=1e-10, switch_diis_err=1e-5, max_iter=100,
-            diis_size=8):
-        """RHF on the GPU (rijk_scf); returns (E, MO rows, result dict)."""
+            diis_size=8, guess=None):
+        """RHF on the GPU (rijk_scf); guess = (D0, R) with D0 = R^T R (e.g. SystemIntegrals.sad()),
+        None for the core-Hamiltonian start.  Returns (E, MO rows, result dict)."""
         n = self.n
         o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1e-10)
+        if guess is not None:
+            gD, gR = _c(guess[0]), _c(guess[1])
+            o.guess_dm, o.guess_rows, o.guess_nrows = _p(gD), _p(gR), gR.shape[0]
         r = ScfResult()
         MO = np.zeros((n, n))
-        self._check(lib().rijk_scf(self._h, _p(_c(H)), _p(_c(S)), int(n_c), float(e_nuc), ctypes.byref(o), _p(MO),
-                                   ctypes.byref(r)))
-        return r.energy, MO, {k: getattr(r, k) for k, _ in ScfResult._fields_}
+        rc = lib().rijk_scf(self._h, _p(_c(H)), _p(_c(S)), int(n_c), float(e_nuc), ctypes.byref(o), _p(MO),
+                            ctypes.byref(r))
+        if rc != ERR_CONVERGE:  # not converged: the result (converged = 0) and its trace are returned
+            self._check(rc)
+        out = {k: getattr(r, k) for k, _ in ScfResult._fields_ if not k.startswith("history")}
+        k = r.history_len
+        out["history"] = [(r.history_energy[i], r.history_diis_err[i], r.history_mixed[i]) for i in range(k)]
+        return r.energy, MO, out
 
     def grad(self, MO, n_c, H, e_nuc, want_3c=False, want_metric=False):
         """(E, dE/dMO (n_c x n), dE/d(P|mu nu) packed [pair][P] or None, dE/d(P|Q) or None)."""

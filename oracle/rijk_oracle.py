@@ -175,22 +175,27 @@ def adjoint_reference(I3_packed, M, H, MO, n_c, Enuc):
 
 
 # --------------------------------------------------------------------- SCF ------
-def scf_rhf(S, H, RI_AA, Vm05, n_occ, Enuc, conv_dm=1e-10, max_iter=100, diis_n=8, jk=None):
+def scf_rhf(S, H, RI_AA, Vm05, n_occ, Enuc, conv_dm=1e-10, max_iter=100, diis_n=8, jk=None, guess=None):
     """Restricted HF with DIIS on F D S - S D F, using the reference's J/K, F and E
-    conventions.  Returns (E, MO, DM, F, iterations).  `jk(DM, MO) -> (J, K)` overrides the
-    Fock build (default: dm_to_f_transform_ri on RI_AA/Vm05)."""
+    conventions.  Returns (E, MO, DM, F, iterations).  `jk(DM, MO, n_rows) -> (J, K)` overrides
+    the Fock build (default: dm_to_f_transform_ri on RI_AA/Vm05); `guess = (D0, R)` starts from
+    the Fock matrix of D0 = R^T R instead of the core Hamiltonian."""
     n = S.shape[0]
     s, U = np.linalg.eigh(S)
     keep = s > 1e-10
     X = U[:, keep] / np.sqrt(s[keep])
     if jk is None:
-        jk = lambda D, MO: dm_to_f_transform_ri(RI_AA, Vm05, D, MO, n_occ, n)
+        jk = lambda D, MO, nr=n_occ: dm_to_f_transform_ri(RI_AA, Vm05, D, MO, nr, n)
 
     def diag(F):
         e, Cp = np.linalg.eigh(X.T @ F @ X)
         return (X @ Cp).T  # rows are orbitals
 
-    MO = diag(H)
+    if guess is not None:
+        J0, K0 = jk(guess[0], guess[1], guess[1].shape[0])
+        MO = diag(calc_f_ao(H, J0, K0))
+    else:
+        MO = diag(H)
     DM = gen_hf_dm(MO, n, n_occ)
     focks, errs = [], []
     E = 0.0

@@ -58,7 +58,7 @@ def test_mixed_k_water_hexamer():
     assert ex < 1e-4
 
 
-@pytest.mark.parametrize("n,naux,nocc", [(200, 96, 97), (64, 40, 16), (150, 70, 1)])
+@pytest.mark.parametrize("n,naux,nocc", [(200, 96, 97), (64, 40, 16), (150, 70, 1), (200, 96, 161), (260, 48, 192)])
 def test_mixed_k_ragged_random(n, naux, nocc):
     rng = np.random.default_rng(n)
     A = rng.normal(size=(naux, naux))

@@ -98,7 +98,8 @@ def _random_problem(n, naux, seed):
     return V, I3
 
 
-@pytest.mark.parametrize("n,naux,nocc", [(70, 100, 13), (64, 33, 16), (1, 5, 1), (130, 257, 0), (200, 96, 97)])
+@pytest.mark.parametrize("n,naux,nocc", [(70, 100, 13), (64, 33, 16), (1, 5, 1), (130, 257, 0), (200, 96, 97),
+                                         (200, 96, 161), (180, 40, 130), (300, 64, 282)])
 def test_jk_parity_ragged_random(n, naux, nocc):
     V, I3 = _random_problem(n, naux, n + naux)
     rng = np.random.default_rng(7)
@@ -136,7 +137,7 @@ def test_errors_are_status_codes_not_crashes():
         assert e.value.code == rijk.ERR_ARG
         fb.set_3c(I3, 8)
         with pytest.raises(rijk.RijkError) as e:
-            fb.dm_to_f_transform_ri(np.eye(8), np.eye(8), 9)  # n_c > n_ao
+            fb.dm_to_f_transform_ri(np.eye(8), np.eye(8), 17)  # n_c beyond n_ao (padded to 16)
         assert e.value.code == rijk.ERR_ARG
         with pytest.raises(rijk.RijkError) as e:
             fb.dm_to_f_transform_ri(np.eye(8), np.eye(8), 2, precision=5)

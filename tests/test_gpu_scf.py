@@ -27,7 +27,9 @@ def test_gpu_scf_reproduces_reference_energy(name):
         fb.set_metric(si.V)
         fb.set_3c(si.I3, si.n)
         E, MO, r = fb.scf(si.H, si.S, si.nocc, si.Enuc)
-    assert r["converged"] == 1
+        Eg, _, rg = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=si.sad())
+    assert r["converged"] == 1 and rg["converged"] == 1
+    assert abs(Eg - E) < 1e-9
     assert abs(E - p["energy"]) < 2e-9, (E, p["energy"])
     # orbitals are S-orthonormal, one per row as the reference's MO_VEC
     C = MO[:r["nmo"]]
@@ -48,3 +50,22 @@ def test_gpu_scf_mixed_then_fp64_matches_fp64():
     Vm05, _ = O.s05_calc(si.V)
     Eo, *_ = O.scf_rhf(si.S, si.H, O.unpack_3c(si.I3, si.n), Vm05, si.nocc, si.Enuc)
     assert abs(E64 - Eo) < 1e-9
+
+
+def test_gpu_scf_long_alkane_full_size():
+    """C40H82 cc-pVDZ / cc-pVDZ-JKFIT (n = 970, naux = 4686, n_c = 161), from the SAD start:
+    the core-Hamiltonian start diverges for this chain, the SAD start converges; mixed builds
+    followed by FP64 reach the FP64 energy to 1e-8 Eh."""
+    from nopt_b200.molecules import alkane
+    si = ints.SystemIntegrals(alkane(40, 0), "cc-pvdz", "cc-pvdz-jkfit")
+    assert (si.n, si.naux, si.nocc) == (970, 4686, 161)
+    guess = si.sad()
+    with rijk.FockBuilder(0) as fb:
+        fb.set_metric(si.V)
+        fb.set_3c(si.I3, si.n)
+        E64, _, r64 = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess)
+        Em, _, rm = fb.scf(si.H, si.S, si.nocc, si.Enuc, precision=rijk.PREC_MIXED, guess=guess)
+    assert r64["converged"] and rm["converged"]
+    assert rm["iterations_mixed"] > 0
+    assert abs(Em - E64) < 1e-8
+    assert -1562.6 < E64 < -1562.5

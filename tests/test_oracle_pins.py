@@ -105,3 +105,16 @@ def test_three_centre_rotational_invariance_of_fitted_energy():
         E, MO, DM, F, it = O.scf_rhf(si.S, si.H, si.I3, Vm05, si.nocc, si.Enuc)
         out.append(E)
     assert abs(out[0] - out[1]) < 1e-9
+
+
+def test_sad_guess_density_and_factor_rows():
+    """The superposition of atomic densities carries n_occ electron pairs, factors as R^T R and
+    starts the oracle SCF at the reference's C2H4 energy."""
+    p = [q for q in GOLD["pins"] if q["name"] == "c2h4"][0]
+    si = ints.SystemIntegrals(_mol(p), p["basis"], p["aux"], layout=ints.LAYOUT_NOPT_FULL)
+    D0, R = si.sad()
+    assert abs(np.sum(D0 * si.S) - si.nocc) < 1e-10
+    np.testing.assert_allclose(R.T @ R, D0, atol=1e-12)
+    Vm05, _ = O.s05_calc(si.V)
+    E, MO, DM, F, it = O.scf_rhf(si.S, si.H, si.I3, Vm05, si.nocc, si.Enuc, guess=(D0, R))
+    assert abs(E - p["energy"]) < 2e-9
