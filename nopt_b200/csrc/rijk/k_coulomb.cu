@@ -7,6 +7,8 @@
 //                                        summed while unpacking)
 // Both passes stream B once with 128-bit loads that bypass L1; reductions are warp
 // shuffles.  Algorithmic traffic: 2 * |B| bytes per build.
+#include <cuda_bf16.h>
+
 #include "dmma.cuh"
 #include "rijk_internal.h"
 
@@ -111,6 +113,152 @@ void launch_coulomb_j(const double* B, const double* w, long naux, long tile_ele
   long qper = (naux + nsplit - 1) / nsplit;
   dim3 grid(static_cast<unsigned>((tile_elems / 2 + J_THREADS - 1) / J_THREADS), static_cast<unsigned>(nsplit));
   k_coulomb_j<<<grid, J_THREADS, 0, s>>>(B, w, naux, tile_elems, qper, Jpart);
+}
+
+// ---------------------------------------------------------------------------------
+// The same two passes over the split-BF16 copy of B (mixed form): Bmix[Q][t][hl][64][64],
+// hi and lo planes of a tile 4096 elements apart, tiles t < ntile (the padded tile row of an
+// odd tile count is never read).  Each thread takes 8 consecutive elements (16-byte loads of
+// each plane), forms b = hi + lo in fp32 (exact: the planes are 8 bits apart) and
+// accumulates in fp64.  Half the bytes of the FP64 passes; B is represented to ~2^-17.
+
+__device__ __forceinline__ void bf16x8_sum(const uint4 h, const uint4 l, float (&b)[8]) {
+  const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&h);
+  const __nv_bfloat162* lp = reinterpret_cast<const __nv_bfloat162*>(&l);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float2 a = __bfloat1622float2(hp[k]);
+    float2 c = __bfloat1622float2(lp[k]);
+    b[2 * k] = a.x + c.x;
+    b[2 * k + 1] = a.y + c.y;
+  }
+}
+
+__device__ __forceinline__ uint4 ldg_stream_u4(const void* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
+// Element offset of packed element e (tile t = e / 4096) inside one aux function's Bmix block.
+__device__ __forceinline__ long mix_off(long e) { return (e >> 12) * 8192 + (e & 4095); }
+
+constexpr int WM_QB = 8;          // aux functions per CTA (each Dt load serves 8 of them)
+constexpr int WM_THREADS = 256;
+
+__global__ void __launch_bounds__(WM_THREADS) k_coulomb_w_mixed(const __nv_bfloat16* __restrict__ Bmix,
+                                                                 const double* __restrict__ Dt, long naux, long ntile,
+                                                                 long ntile2, double* __restrict__ w) {
+  const long q0 = static_cast<long>(blockIdx.x) * WM_QB;
+  const long n8 = ntile * TILE2 / 8;
+  const long qstride = ntile2 * 2 * TILE2;
+  double acc[WM_QB];  // each group of 8 products is summed in fp32, the groups in fp64
+#pragma unroll
+  for (int j = 0; j < WM_QB; ++j) acc[j] = 0.0;
+  const __nv_bfloat16* qb[WM_QB];
+#pragma unroll
+  for (int j = 0; j < WM_QB; ++j) qb[j] = Bmix + (q0 + j < naux ? q0 + j : naux - 1) * qstride;
+  for (long e8 = threadIdx.x; e8 < n8; e8 += WM_THREADS) {
+    const long e = e8 * 8;
+    const long off = mix_off(e);
+    uint4 h[WM_QB], l[WM_QB];
+#pragma unroll
+    for (int j = 0; j < WM_QB; ++j) {
+      h[j] = ldg_stream_u4(qb[j] + off);
+      l[j] = ldg_stream_u4(qb[j] + off + TILE2);
+    }
+    const double4 d0 = *reinterpret_cast<const double4*>(Dt + e);
+    const double4 d1 = *reinterpret_cast<const double4*>(Dt + e + 4);
+    const float d[8] = {static_cast<float>(d0.x), static_cast<float>(d0.y), static_cast<float>(d0.z),
+                        static_cast<float>(d0.w), static_cast<float>(d1.x), static_cast<float>(d1.y),
+                        static_cast<float>(d1.z), static_cast<float>(d1.w)};
+#pragma unroll
+    for (int j = 0; j < WM_QB; ++j) {
+      float b[8];
+      bf16x8_sum(h[j], l[j], b);
+      float t = 0.f;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) t = fmaf(b[k], d[k], t);
+      acc[j] += static_cast<double>(t);
+    }
+  }
+  __shared__ double red[WM_QB][WM_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < WM_QB; ++j) {
+    double v = warp_sum(acc[j]);
+    if (lane == 0) red[j][warp] = v;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int j = 0; j < WM_QB; ++j) {
+      double v = lane < WM_THREADS / 32 ? red[j][lane] : 0.0;
+      v = warp_sum(v);
+      if (lane == 0 && q0 + j < naux) w[q0 + j] = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(J_THREADS) k_coulomb_j_mixed(const __nv_bfloat16* __restrict__ Bmix,
+                                                                const double* __restrict__ w, long naux, long ntile,
+                                                                long ntile2, long qper, double* __restrict__ Jpart) {
+  const long e8 = static_cast<long>(blockIdx.x) * J_THREADS + threadIdx.x;
+  const long s = blockIdx.y;
+  const long tile_elems = ntile * TILE2;
+  if (e8 * 8 >= tile_elems) return;
+  const long qa = s * qper;
+  const long qb = qa + qper < naux ? qa + qper : naux;
+  const long qstride = ntile2 * 2 * TILE2;
+  const __nv_bfloat16* base = Bmix + mix_off(e8 * 8);
+  double acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+  long q = qa;
+  for (; q + 4 <= qb; q += 4) {
+    uint4 h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const __nv_bfloat16* p = base + (q + u) * qstride;
+      h[u] = ldg_stream_u4(p);
+      l[u] = ldg_stream_u4(p + TILE2);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      float b[8];
+      bf16x8_sum(h[u], l[u], b);
+      const double wq = __ldg(w + q + u);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] = fma(static_cast<double>(b[k]), wq, acc[k]);
+    }
+  }
+  for (; q < qb; ++q) {
+    const __nv_bfloat16* p0 = base + q * qstride;
+    float b0[8];
+    bf16x8_sum(ldg_stream_u4(p0), ldg_stream_u4(p0 + TILE2), b0);
+    const double w0 = __ldg(w + q);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] = fma(static_cast<double>(b0[k]), w0, acc[k]);
+  }
+  double* out = Jpart + s * tile_elems + e8 * 8;
+  *reinterpret_cast<double4*>(out) = make_double4(acc[0], acc[1], acc[2], acc[3]);
+  *reinterpret_cast<double4*>(out + 4) = make_double4(acc[4], acc[5], acc[6], acc[7]);
+}
+
+void launch_coulomb_w_mixed(const __nv_bfloat16* Bmix, const double* Dt, long naux, long ntile, long ntile2, double* w,
+                            cudaStream_t s) {
+  unsigned grid = static_cast<unsigned>((naux + WM_QB - 1) / WM_QB);
+  k_coulomb_w_mixed<<<grid, WM_THREADS, 0, s>>>(Bmix, Dt, naux, ntile, ntile2, w);
+}
+
+void launch_coulomb_j_mixed(const __nv_bfloat16* Bmix, const double* w, long naux, long ntile, long ntile2,
+                            int nsplit, double* Jpart, cudaStream_t s) {
+  const long tile_elems = ntile * TILE2;
+  long qper = (naux + nsplit - 1) / nsplit;
+  dim3 grid(static_cast<unsigned>((tile_elems / 8 + J_THREADS - 1) / J_THREADS), static_cast<unsigned>(nsplit));
+  k_coulomb_j_mixed<<<grid, J_THREADS, 0, s>>>(Bmix, w, naux, ntile, ntile2, qper, Jpart);
 }
 
 }  // namespace rijk

@@ -601,7 +601,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   k_syrk_tc<<<grid, kTcThreads, smem, s>>>(mX, sp);
   ++launches;
   prof_mark(ctx, "syrk_tc");
-  launch_unpack_sym(static_cast<const double*>(ctx->Kpart.p), nsplit, ntile2, n, dK, s);
+  launch_unpack_sym(static_cast<double*>(ctx->Kpart.p), nsplit, ntile2, n, dK, s);
   ++launches;
   prof_mark(ctx, "unpack_k");
   ctx->stats.kernels_last_fock = launches;

@@ -38,23 +38,40 @@ __global__ void k_pack_mo(const double* __restrict__ MO, long nocc, long n, long
   }
 }
 
-// out[mu][nu] = sum_s partial[s][tile(max,min)][r][c] with (r, c) oriented to the stored tile.
-__global__ void k_unpack_sym(const double* __restrict__ partial, int nsplit, long ntile, long n,
-                             double* __restrict__ out) {
+// Two steps: (1) sum the split partials into the first split's slot (each element read and
+// written by one thread, coalesced); (2) one CTA per 32 x 32 block of the full square copies
+// the stored tile block, transposing it through shared memory for the upper triangle.
+__global__ void k_sum_splits(double* __restrict__ partial, int nsplit, long ntile) {
+  const long total = ntile * TILE2;
+  const long sstride = total;
   long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  long total = n * n;
   for (; idx < total; idx += static_cast<long>(gridDim.x) * blockDim.x) {
-    long mu = idx / n, nu = idx % n;
-    long I = mu / TILE, J = nu / TILE;
-    long r = mu % TILE, c = nu % TILE;
-    if (I < J) {
-      long tmp = I; I = J; J = tmp;
-      tmp = r; r = c; c = tmp;
-    }
-    const double* p = partial + tri_index(I, J) * TILE2 + r * TILE + c;
-    double v = 0.0;
-    for (int s = 0; s < nsplit; ++s) v += p[static_cast<long>(s) * ntile * TILE2];
-    out[idx] = v;
+    double v = partial[idx];
+    for (int s = 1; s < nsplit; ++s) v += partial[static_cast<long>(s) * sstride + idx];
+    partial[idx] = v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_unpack_blocks(const double* __restrict__ packed, long n, long nb,
+                                                      double* __restrict__ out) {
+  __shared__ double blk[32][33];
+  const long bi = blockIdx.x / nb, bj = blockIdx.x % nb;  // 32-blocks of the output
+  const long I = bi / 2, J = bj / 2;                       // 64-tiles
+  const bool lower = I >= J;
+  // stored tile (max, min); sub-block of it that holds this output block
+  const long a = lower ? I : J, b = lower ? J : I;
+  const long rs = lower ? (bi & 1) * 32 : (bj & 1) * 32;  // row offset inside the stored tile
+  const long cs = lower ? (bj & 1) * 32 : (bi & 1) * 32;
+  const double* src = packed + tri_index(a, b) * TILE2;
+  for (int e = threadIdx.x; e < 1024; e += 256) {
+    const int r = e / 32, c = e % 32;
+    blk[r][c] = src[(rs + r) * TILE + cs + c];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 1024; e += 256) {
+    const int r = e / 32, c = e % 32;
+    const long mu = bi * 32 + r, nu = bj * 32 + c;
+    if (mu < n && nu < n) out[mu * n + nu] = lower ? blk[r][c] : blk[c][r];
   }
 }
 
@@ -81,8 +98,12 @@ void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, 
   k_pack_mo<<<grid_for(noccp * npad, 256), 256, 0, s>>>(MO, nocc, n, noccp, npad, MOp);
 }
 
-void launch_unpack_sym(const double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s) {
-  k_unpack_sym<<<grid_for(n * n, 256), 256, 0, s>>>(partial, nsplit, ntile, n, out);
+// Sums the split partials in place (into split 0) and writes the full symmetric n x n matrix.
+void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s) {
+  double* p = partial;
+  if (nsplit > 1) k_sum_splits<<<grid_for(ntile * TILE2, 256), 256, 0, s>>>(p, nsplit, ntile);
+  const long nb = (n + 31) / 32;
+  k_unpack_blocks<<<static_cast<unsigned>(nb * nb), 256, 0, s>>>(p, n, nb, out);
 }
 
 void launch_scan_nonfinite(const double* x, long count, int* err, cudaStream_t s) {

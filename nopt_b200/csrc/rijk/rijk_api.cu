@@ -144,17 +144,30 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
       (rc = ensure(ctx, ctx->w, naux * sizeof(double), "w")) ||
       (rc = ensure(ctx, ctx->Jpart, static_cast<size_t>(nsJ) * tile_elems * sizeof(double), "Jpart")))
     return rc;
+  if (precision == RIJK_PREC_MIXED && (rc = mixed_prepare(ctx))) return rc;
   cudaEventRecord(ctx->ev0, s);
   prof_begin(ctx);
   launch_pack_density(dD, n, npad, nt, static_cast<double*>(ctx->Dt.p), s);
   prof_mark(ctx, "pack_density");
-  launch_coulomb_w(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->Dt.p), naux, tile_elems,
-                   static_cast<double*>(ctx->w.p), s);
-  prof_mark(ctx, "coulomb_w");
-  launch_coulomb_j(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->w.p), naux, tile_elems, nsJ,
-                   static_cast<double*>(ctx->Jpart.p), s);
-  prof_mark(ctx, "coulomb_j");
-  launch_unpack_sym(static_cast<const double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, s);
+  if (precision == RIJK_PREC_MIXED) {
+    // mixed form: both passes over the split-BF16 copy (half the bytes of the FP64 passes)
+    const long ntile2 = round_up(nt, 2) * (round_up(nt, 2) + 1) / 2;
+    const __nv_bfloat16* Bm = static_cast<const __nv_bfloat16*>(ctx->Bmix.p);
+    launch_coulomb_w_mixed(Bm, static_cast<const double*>(ctx->Dt.p), naux, ntile, ntile2,
+                           static_cast<double*>(ctx->w.p), s);
+    prof_mark(ctx, "coulomb_w_mixed");
+    launch_coulomb_j_mixed(Bm, static_cast<const double*>(ctx->w.p), naux, ntile, ntile2, nsJ,
+                           static_cast<double*>(ctx->Jpart.p), s);
+    prof_mark(ctx, "coulomb_j_mixed");
+  } else {
+    launch_coulomb_w(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->Dt.p), naux, tile_elems,
+                     static_cast<double*>(ctx->w.p), s);
+    prof_mark(ctx, "coulomb_w");
+    launch_coulomb_j(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->w.p), naux, tile_elems,
+                     nsJ, static_cast<double*>(ctx->Jpart.p), s);
+    prof_mark(ctx, "coulomb_j");
+  }
+  launch_unpack_sym(static_cast<double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, s);
   prof_mark(ctx, "unpack_j");
   launches += 4;
   cudaEventRecord(ctx->ev1, s);
@@ -181,7 +194,7 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
     launch_syrk_f64(static_cast<const double*>(ctx->XT.p), npad, nt, kdim, nsK, static_cast<double*>(ctx->Kpart.p),
                     s);
     prof_mark(ctx, "syrk_f64");
-    launch_unpack_sym(static_cast<const double*>(ctx->Kpart.p), nsK, ntile, n, dK, s);
+    launch_unpack_sym(static_cast<double*>(ctx->Kpart.p), nsK, ntile, n, dK, s);
     prof_mark(ctx, "unpack_k");
     launches += 4;
   }
@@ -191,7 +204,8 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
   const double noccd = static_cast<double>(nocc);
   ctx->stats.flops_last_fock = 4.0 * static_cast<double>(tile_elems) * naux +
                                2.0 * noccd * npad * npad * naux + static_cast<double>(npad) * (npad + TILE) * noccd * naux;
-  ctx->stats.bytes_last_fock = 2.0 * static_cast<double>(tile_elems) * naux * sizeof(double);
+  ctx->stats.bytes_last_fock = 2.0 * static_cast<double>(tile_elems) * naux *
+                               (precision == RIJK_PREC_MIXED ? 2 * sizeof(__nv_bfloat16) : sizeof(double));
   ctx->stats.kernels_last_fock = launches;
   prof_collect(ctx);
   return RIJK_OK;

@@ -14,6 +14,7 @@
 // half-transformed tensor with the contraction index k = (Q, i) contiguous.
 #pragma once
 #include <cublas_v2.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
@@ -97,7 +98,7 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
 // ---- k_pack.cu
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s);
-void launch_unpack_sym(const double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s);
+void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s);
 void launch_scan_nonfinite(const double* x, long count, int* err, cudaStream_t s);
 
 // ---- k_metric.cu
@@ -110,6 +111,12 @@ int coulomb_nsplit(long tile_elems, long naux);
 void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s);
 void launch_coulomb_j(const double* B, const double* w, long naux, long tile_elems, int nsplit, double* Jpart,
                       cudaStream_t s);
+
+// Mixed form: the same passes over the split-BF16 copy (Bmix[Q][t][hl][64][64], ntile2 tiles per Q).
+void launch_coulomb_w_mixed(const __nv_bfloat16* Bmix, const double* Dt, long naux, long ntile, long ntile2, double* w,
+                            cudaStream_t s);
+void launch_coulomb_j_mixed(const __nv_bfloat16* Bmix, const double* w, long naux, long ntile, long ntile2,
+                            int nsplit, double* Jpart, cudaStream_t s);
 
 // ---- k_exchange_f64.cu
 void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s);
