@@ -30,6 +30,11 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernels,
+# from one ncu capture each (profiles/k_xform_f64_h2o16_dz.md, profiles/k_xform_tc_syrk_tc_h2o16_dz.md).
+NCU_TRAFFIC = {("h2o16_dz", "xform_f64"): 1.277519e9 + 0.439185e9,
+               ("h2o16_dz", "xform_tc"): 0.639804e9 + 0.199220e9,
+               ("h2o16_dz", "syrk_tc"): 0.228556e9 + 0.047133e9}
 WORKLOAD_NAMES = {"h2o6_dz": "(H2O)6 cc-pVDZ/cc-pVDZ-JKFIT", "h2o16_dz": "(H2O)16 cc-pVDZ/cc-pVDZ-JKFIT",
                   "c40h82_dz": "C40H82 cc-pVDZ/cc-pVDZ-JKFIT", "h2o32_tz": "(H2O)32 cc-pVTZ/cc-pVTZ-JKFIT"}
 METRIC = "RI-JK Fock builds/s (FP64 drop-in; mixed and SCF time beside it)"
@@ -307,7 +312,9 @@ def main():
     else:
         achieved = amount / (stage_ms[top] * 1e-3) / 1e12
         roof = {"kernel": top, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak, "traffic": None,
+                "frac": achieved / fp64_peak, "traffic": NCU_TRAFFIC.get((args.workload, top)),
+                "traffic_note": "bytes per launch from one ncu capture (profiles/); algorithmic: read B once, "
+                                "write XT once = %.3e" % (tile_elems * naux * 8.0 + npad * naux * noccp * 8.0),
                 "peak_source": "FP64 DMMA: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)"}
     cw = stage_ms.get("coulomb_w", 0.0) + stage_ms.get("coulomb_j", 0.0)
     coul = {"achieved_gbs": 2 * tile_elems * naux * 8.0 / (cw * 1e-3) / 1e9 if cw else None, "peak_gbs": hbm}
@@ -330,6 +337,8 @@ def main():
                  "exchange_energy_err": float(abs(np.sum(DM * (Km - K64)))),
                  "stage_ms": mstages, "top_kernel": mtop,
                  "gpu_launches": fb.stats()["kernels_last_fock"] * args.steps}
+        if mtop in ("xform_tc", "syrk_tc"):
+            mixed["traffic"] = NCU_TRAFFIC.get((args.workload, mtop))
         if mtop == "xform_tc":
             fl = 3 * 2.0 * noccp * (npad2 := ((npad + 127) // 128) * 128) * npad2 * naux
             mixed["roofline"] = {"kernel": "xform_tc", "bound": "tensor",
@@ -351,7 +360,8 @@ def main():
         t0 = time.perf_counter()
         guess = si.sad()  # superposition of atomic densities (host, once per geometry)
         t_guess = time.perf_counter() - t0
-        fb.scf(si.H, si.S, nocc, si.Enuc, precision=rijk.PREC_MIXED, guess=guess)  # untimed: first-call set-up
+        for prec in (rijk.PREC_FP64, rijk.PREC_MIXED):  # untimed: first-call set-up of both forms
+            fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, guess=guess)
         for name, prec in (("fp64", rijk.PREC_FP64), ("mixed_then_fp64", rijk.PREC_MIXED)):
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()

@@ -125,6 +125,8 @@ typedef struct {
   double switch_diis_err; /* default 1e-5; the switch also happens when the mixed-phase error has
                              not improved for 5 iterations or after max_iter / 2 mixed iterations */
   int diis_size;          /* default 8                                                          */
+  int diis_keep_on_switch; /* 0 (default): restart DIIS at the switch to FP64 (measured faster);
+                             1: keep the mixed-phase vectors until the history rolls over       */
   double lindep;          /* overlap eigenvalues below this are dropped; default 1e-10           */
   /* Optional start (host arrays): a density D0 (n x n) with factor rows R (guess_nrows x n),
    * D0 = R^T R, e.g. a superposition of atomic densities; its FP64 Fock build replaces the

@@ -10,6 +10,8 @@
 //   K4  K[mu][nu] = sum_k XT[mu][k] XT[nu][k], k = (Q, i): only the lower tiles (a >= b)
 //       are formed, split over k into nsplit ranges whose partial tiles are summed (and
 //       mirrored) by the unpack kernel.  FLOPs n(n+1) noccp naux, the SYRK count.
+#include <algorithm>
+
 #include "gemm_f64.cuh"
 #include "rijk_internal.h"
 
@@ -192,13 +194,26 @@ __global__ void __launch_bounds__(S_THREADS)
   }
 }
 
+// Splits of the contraction range: enough CTAs for about two waves of the 2 CTAs per SM the
+// kernel fits (shared memory), chosen among [s_min, 4 s_min] so the last wave is fullest.
 int syrk_nsplit(long nt, long kdim) {
-  long ntile = nt * (nt + 1) / 2;
-  long want = (148L * 4 + ntile - 1) / ntile;
-  long maxs = kdim / (KC * 8);
-  if (want > maxs) want = maxs;
-  if (want < 1) want = 1;
-  return static_cast<int>(want);
+  const long ntile = nt * (nt + 1) / 2;
+  const long slots = 148L * 2;
+  const long maxs = std::max<long>(1, kdim / (KC * 8));
+  const long need = slots * 19 / 10;
+  const long smin = std::min(maxs, std::max<long>(1, (need + ntile - 1) / ntile));
+  long best = smin;
+  double best_eff = 0.0;
+  for (long sp = smin; sp <= std::min(maxs, 4 * smin); ++sp) {
+    const long ctas = ntile * sp;
+    const long waves = (ctas + slots - 1) / slots;
+    const double eff = static_cast<double>(ctas) / static_cast<double>(waves * slots);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = sp;
+    }
+  }
+  return static_cast<int>(best);
 }
 
 void launch_syrk_f64(const double* XT, long npad, long nt, long kdim, int nsplit, double* Kpart, cudaStream_t s) {

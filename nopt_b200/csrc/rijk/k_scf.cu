@@ -13,6 +13,7 @@
 // and column-major forms coincide; the orbital matrix C (n x nmo, column i = orbital i) has
 // the memory layout of the reference's MO_VEC (row i = orbital i), so its first n_c columns
 // are passed to the Fock build as MO.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -294,14 +295,37 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   const int nmi = static_cast<int>(nm);
   k_scale_cols<<<grid_of(n * nm), 256, 0, s>>>(pU, pW, n, first, nm, pX);
 
-  // diagonalise X^T F X -> C = X V (first nm columns of pC)
-  auto diag = [&](const double* Fm) -> int {
+  // Inside the loop only the n_c occupied orbitals are needed: syevdx for the lowest n_c
+  // eigenpairs (all of them, with syevd, for the final orbitals).
+  const int nev = static_cast<int>(std::max<long>(nocc, 1));
+  int lworkx = 0, meig = 0;
+  if (cusolverDnDsyevdx_bufferSize(cs, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER, nmi,
+                                   pU, nmi, 0.0, 0.0, 1, nev, &meig, pW, &lworkx) != CUSOLVER_STATUS_SUCCESS)
+    return fail(RIJK_ERR_SOLVER, "syevdx buffer query failed");
+  if (lworkx > lwork) {
+    if ((rc = ensure(ctx, work, static_cast<size_t>(lworkx) * sizeof(double), "scf syevdx work"))) {
+      cleanup();
+      return rc;
+    }
+    pWork = static_cast<double*>(work.p);
+  }
+  // diagonalise X^T F X -> C = X V (first nm columns of pC, or the first n_c when partial)
+  auto diag = [&](const double* Fm, bool all = false) -> int {
     cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, Fm, ni, pX, ni, &zero, pT1, ni);    // F X
     cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT1, ni, &zero, pU, nmi);  // X^T F X
-    if (cusolverDnDsyevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nmi, pU, nmi, pW, pWork, lwork,
-                         pInfo) != CUSOLVER_STATUS_SUCCESS)
-      return RIJK_ERR_SOLVER;
-    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, nmi, &one, pX, ni, pU, nmi, &zero, pC, ni);   // C = X V
+    int ncols = nmi;
+    if (all) {
+      if (cusolverDnDsyevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nmi, pU, nmi, pW, pWork, lwork,
+                           pInfo) != CUSOLVER_STATUS_SUCCESS)
+        return RIJK_ERR_SOLVER;
+    } else {
+      if (cusolverDnDsyevdx(cs, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER, nmi, pU, nmi,
+                            0.0, 0.0, 1, nev, &meig, pW, pWork, std::max(lwork, lworkx), pInfo) !=
+          CUSOLVER_STATUS_SUCCESS)
+        return RIJK_ERR_SOLVER;
+      ncols = nev;
+    }
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ncols, nmi, &one, pX, ni, pU, nmi, &zero, pC, ni);  // C = X V
     return RIJK_OK;
   };
   auto density = [&](double* Dm) {  // D = C_occ C_occ^T
@@ -402,10 +426,13 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       stalled = since_best >= 5 || nmix >= o.max_iter / 2;
     }
     if (prec == RIJK_PREC_MIXED && (err < o.switch_diis_err || stalled)) {
-      // switch to the FP64 form: rebuild F for this same density and restart DIIS
+      // switch to the FP64 form: rebuild F for this same density and restart DIIS (unless the
+      // caller keeps the mixed-phase vectors)
       prec = RIJK_PREC_FP64;
-      m = 0;
-      head = 0;
+      if (!o.diis_keep_on_switch) {
+        m = 0;
+        head = 0;
+      }
       --it;
       continue;
     }
@@ -461,7 +488,12 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   }
   reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
   cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (MO) cudaMemcpyAsync(MO, pC, static_cast<size_t>(nm) * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (MO) {
+    // orbitals of the final Fock matrix (all of them), as the reference's closing diagonalisation
+    // (src/SCF.cpp:178)
+    if (diag(pF, true) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the final Fock matrix failed");
+    cudaMemcpyAsync(MO, pC, static_cast<size_t>(nm) * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  }
   if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf final")) || (rc = check_device_error(ctx))) {
     cleanup();
     return rc;

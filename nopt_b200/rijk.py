@@ -41,7 +41,8 @@ class Stats(ctypes.Structure):
 
 class ScfOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv_dm_rms", ctypes.c_double), ("precision", ctypes.c_int),
-                ("switch_diis_err", ctypes.c_double), ("diis_size", ctypes.c_int), ("lindep", ctypes.c_double),
+                ("switch_diis_err", ctypes.c_double), ("diis_size", ctypes.c_int),
+                ("diis_keep_on_switch", ctypes.c_int), ("lindep", ctypes.c_double),
                 ("guess_dm", _dp), ("guess_rows", _dp), ("guess_nrows", ctypes.c_long)]
 
 
@@ -166,11 +167,12 @@ class FockBuilder:
         self._check(lib().rijk_fock_device(self._h, _vp(dD), _vp(dMO), int(n_c), _vp(dJ), _vp(dK), precision))
 
     def scf(self, H, S, n_c, e_nuc, precision=PREC_FP64, conv_dm_rms=1e-10, switch_diis_err=1e-5, max_iter=100,
-            diis_size=8, guess=None):
+            diis_size=8, guess=None, diis_keep_on_switch=False):
         """RHF on the GPU (rijk_scf); guess = (D0, R) with D0 = R^T R (e.g. SystemIntegrals.sad()),
         None for the core-Hamiltonian start.  Returns (E, MO rows, result dict)."""
         n = self.n
-        o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1e-10)
+        o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1 if diis_keep_on_switch else 0,
+                    1e-10)
         if guess is not None:
             gD, gR = _c(guess[0]), _c(guess[1])
             o.guess_dm, o.guess_rows, o.guess_nrows = _p(gD), _p(gR), gR.shape[0]
