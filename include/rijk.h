@@ -83,6 +83,13 @@ int rijk_get_stats(const rijk_ctx* ctx, rijk_stats_t* out);
 /* (P|Q), naux x naux host array.  Factorises the metric on the GPU in FP64. */
 int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int metric_form);
 
+/* Hold only the aux functions [q0, q1) of the fitted tensor (call after rijk_set_metric,
+ * before rijk_set_3c).  J, K and rijk_mo_ints are sums over the aux index, so a Fock build of
+ * such a context returns the slice's partial J and K; contexts on several GPUs that cover
+ * [0, naux) give the full J and K after one all-reduce (sum).  rijk_scf and rijk_grad need
+ * the whole range. */
+int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1);
+
 /* Three-centre integrals (host array, layout RIJK_LAYOUT_*).  Forms the fitted tensor
  * B^Q_{mu nu} = sum_P M_QP (P|mu nu) on the GPU, stored packed (mu >= nu) in HBM. */
 int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n_ao, long naux, int layout);
@@ -163,6 +170,15 @@ typedef struct {
  * reference's MO_VEC; E as in src/SCF.cpp:134. */
 int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long n_c, double e_nuc, const rijk_scf_opts_t* opts,
              double* MO, rijk_scf_result_t* result);
+
+/* Drop-in for calc_2el_MO_INTS_RI(n_ao, DM_D, J, K, MO_INTS, MO_VEC, MO_VEC1, MO_VEC2, n_c, n_a, t)
+ * (src/RI.cpp:178-292; the CASSCF call at src/CAS.cpp:461): the active-space integrals
+ *   MO_INTS[(b n_a + a) n_a^2 + d n_a + c] = sum_Q (C1 B^Q C2^T)_ab (C1 B^Q C2^T)_cd
+ * with C1 = MO_VEC1, C2 = MO_VEC2 (n_a orbitals as rows, or as columns of an n_ao x n_a array
+ * when t != 0), then, unless J or K is NULL, the core J and K of DM_D and the first n_c rows
+ * of MO_VEC (as rijk_fock).  Host pointers; synchronous; FP64. */
+int rijk_mo_ints(rijk_ctx* ctx, const double* DM_D, double* J, double* K, double* MO_INTS, const double* MO_VEC,
+                 const double* MO_VEC1, const double* MO_VEC2, long n_c, long n_a, long t);
 
 /* Adjoint of the Fock build (no reference counterpart; the reference differentiates by finite
  * differences, src/QM_calc.cpp:142).  For the orbitals MO (n_c rows of n, host) and D = C^T C:

@@ -26,6 +26,7 @@ CUDA_SOURCES = [
     "rijk/k_exchange_tc.cu",
     "rijk/k_scf.cu",
     "rijk/k_adjoint.cu",
+    "rijk/k_moints.cu",
     "rijk/rijk_noalloc.cu",
 ]
 

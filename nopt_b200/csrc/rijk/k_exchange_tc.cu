@@ -524,10 +524,10 @@ int mixed_prepare(rijk_ctx* ctx) {
   if (ctx->have_bmix) return RIJK_OK;
   if (!encode_fn()) return set_err(ctx, RIJK_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
   const long nt2 = round_up(ctx->nt, 2), ntile2 = nt2 * (nt2 + 1) / 2;
-  const size_t bytes = static_cast<size_t>(ctx->naux) * ntile2 * 2 * TILE2 * sizeof(__nv_bfloat16);
+  const size_t bytes = static_cast<size_t>(ctx->nq) * ntile2 * 2 * TILE2 * sizeof(__nv_bfloat16);
   int rc = ensure(ctx, ctx->Bmix, bytes, "split-bf16 copy of B");
   if (rc) return rc;
-  dim3 grid(static_cast<unsigned>(ntile2), static_cast<unsigned>(ctx->naux));
+  dim3 grid(static_cast<unsigned>(ntile2), static_cast<unsigned>(ctx->nq));
   k_split_b<<<grid, 256, 0, ctx->stream>>>(static_cast<const double*>(ctx->B.p), ctx->nt, ctx->ntile, ntile2,
                                            static_cast<__nv_bfloat16*>(ctx->Bmix.p));
   rc = cuda_check(ctx, cudaGetLastError(), "split copy of B");
@@ -540,7 +540,7 @@ int mixed_prepare(rijk_ctx* ctx) {
 int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   int rc = mixed_prepare(ctx);
   if (rc) return rc;
-  const long n = ctx->n, naux = ctx->naux;
+  const long n = ctx->n, naux = ctx->nq;
   const long nt2 = round_up(ctx->nt, 2), ntile2 = nt2 * (nt2 + 1) / 2, npad2 = nt2 * TILE;
   const long noccp = round_up(nocc, 16);
   const long kdim = naux * noccp;

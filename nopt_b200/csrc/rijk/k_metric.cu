@@ -17,8 +17,9 @@ namespace rijk {
 constexpr int K1_THREADS = 128;
 
 __global__ void __launch_bounds__(K1_THREADS)
-    k_metric_contract(const double* __restrict__ M, long nauxp, const double* __restrict__ I3, int layout, long n,
-                      long naux, long I0, long t0, long rows_in_chunk_base, double* __restrict__ B, long tile_elems) {
+    k_metric_contract(const double* __restrict__ M, long nauxp, long mrows, const double* __restrict__ I3, int layout,
+                      long n, long naux, long I0, long t0, long rows_in_chunk_base, double* __restrict__ B,
+                      long tile_elems) {
   extern __shared__ __align__(16) double smem_k1[];
   double* sA[2] = {smem_k1, smem_k1 + 64 * LDK};
   double* sB[2] = {smem_k1 + 2 * 64 * LDK, smem_k1 + 3 * 64 * LDK};
@@ -57,7 +58,7 @@ __global__ void __launch_bounds__(K1_THREADS)
       int row = idx >> 4, seg = idx & 15;
       long q = q0 + row;
       const double* src = M + q * nauxp + p0 + seg * 2;
-      cp_async16(&sA[stage][row * LDK + seg * 2], q < nauxp ? src : M, q < nauxp);
+      cp_async16(&sA[stage][row * LDK + seg * 2], q < mrows ? src : M, q < mrows);
       long ro = rowoff[row];
       const double* srcb = I3 + (ro >= 0 ? ro : 0) * nauxp + p0 + seg * 2;
       cp_async16(&sB[stage][row * LDK + seg * 2], srcb, ro >= 0);
@@ -98,8 +99,8 @@ __global__ void __launch_bounds__(K1_THREADS)
 
 // I3 holds the tile rows I in [I0, I1): full layout rows (mu - I0*64)*n + nu, packed layout
 // pair rows starting at pair_base = (I0*64)(I0*64+1)/2.
-void launch_metric_contract_chunk(const double* M, long nauxp, const double* I3, int layout, long n, long naux,
-                                  long nt, long I0, long I1, double* B, cudaStream_t s) {
+void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const double* I3, int layout, long n,
+                                  long naux, long nt, long I0, long I1, double* B, cudaStream_t s) {
   long t0 = tri_index(I0, 0);
   long t1 = tri_index(I1, 0);
   long ntile = nt * (nt + 1) / 2;
@@ -112,8 +113,8 @@ void launch_metric_contract_chunk(const double* M, long nauxp, const double* I3,
     cudaFuncSetAttribute(k_metric_contract, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     attr = true;
   }
-  k_metric_contract<<<grid, K1_THREADS, smem, s>>>(M, nauxp, I3, layout, n, naux, I0, t0, pair_base, B,
-                                                 ntile * TILE2);
+  k_metric_contract<<<grid, K1_THREADS, smem, s>>>(M, nauxp, mrows, I3, layout, n, naux, I0, t0, pair_base, B,
+                                                   ntile * TILE2);
 }
 
 }  // namespace rijk

@@ -196,6 +196,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   if (o.diis_size > 32) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: diis_size above 32");
   if (o.guess_dm && (!o.guess_rows || o.guess_nrows <= 0 || o.guess_nrows > round_up(ctx->n, 16)))
     return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: guess needs factor rows (1 .. n_ao of them)");
+  if (ctx->nq != ctx->naux)
+    return set_err(ctx, RIJK_ERR_STATE, "rijk_scf needs all aux functions in one context (no aux range)");
   cudaSetDevice(ctx->device);
   const auto t_start = std::chrono::steady_clock::now();
   const long n = ctx->n, nn = n * n;

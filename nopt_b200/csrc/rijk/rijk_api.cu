@@ -16,8 +16,6 @@
 
 namespace rijk {
 
-void launch_metric_contract_chunk(const double* M, long nauxp, const double* I3, int layout, long n, long naux,
-                                  long nt, long I0, long I1, double* B, cudaStream_t s);
 int mixed_prepare(rijk_ctx* ctx);
 int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK);
 
@@ -134,7 +132,8 @@ static void prof_collect(rijk_ctx* ctx) {
 
 int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
                      int precision) {
-  const long n = ctx->n, naux = ctx->naux, nt = ctx->nt, npad = ctx->npad, ntile = ctx->ntile;
+  // naux here is the number of aux functions this context holds (a slice under rijk_set_aux_range)
+  const long n = ctx->n, naux = ctx->nq, nt = ctx->nt, npad = ctx->npad, ntile = ctx->ntile;
   const long tile_elems = ntile * TILE2;
   cudaStream_t s = ctx->stream;
   int rc;
@@ -307,6 +306,18 @@ RIJK_API int rijk_get_stats(const rijk_ctx* ctx, rijk_stats_t* out) {
   return RIJK_OK;
 }
 
+RIJK_API int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1) {
+  if (!ctx) return RIJK_ERR_ARG;
+  if (!ctx->have_metric) return set_err(ctx, RIJK_ERR_STATE, "rijk_set_aux_range: call rijk_set_metric first");
+  if (q0 < 0 || q1 <= q0 || q1 > ctx->naux)
+    return set_err(ctx, RIJK_ERR_ARG, "rijk_set_aux_range: [%ld, %ld) not inside [0, %ld)", q0, q1, ctx->naux);
+  ctx->q0 = q0;
+  ctx->nq = q1 - q0;
+  ctx->have_b = false;
+  ctx->have_bmix = false;
+  return RIJK_OK;
+}
+
 RIJK_API int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int form) {
   if (!ctx) return RIJK_ERR_ARG;
   if (!PQ || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_metric: null (P|Q) or naux <= 0");
@@ -403,6 +414,8 @@ RIJK_API int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int for
                    hinfo[0]);
   ctx->stats.ms_setup_metric = elapsed(ctx->ev0, ctx->ev1);
   ctx->naux = naux;
+  ctx->q0 = 0;
+  ctx->nq = naux;
   ctx->metric_form = form;
   ctx->have_metric = true;
   ctx->have_b = false;
@@ -424,11 +437,12 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
   cudaStream_t s = ctx->stream;
   const long npad = round_up(n, TILE), nt = npad / TILE, ntile = nt * (nt + 1) / 2;
   const long nauxp = round_up(naux, KC);
+  const long nq = ctx->nq, q0 = ctx->q0;
   int rc;
   ctx->have_b = false;
   ctx->have_bmix = false;
   release(ctx->Bmix);
-  if ((rc = ensure(ctx, ctx->B, static_cast<size_t>(naux) * ntile * TILE2 * sizeof(double), "fitted tensor B")))
+  if ((rc = ensure(ctx, ctx->B, static_cast<size_t>(nq) * ntile * TILE2 * sizeof(double), "fitted tensor B")))
     return rc;
   // Raw integrals go up in blocks of whole tile rows, at most ~2 GiB each.
   const double budget = 2.0 * 1024 * 1024 * 1024;
@@ -455,7 +469,7 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
   if ((rc = ensure(ctx, raw, static_cast<size_t>(std::max<long>(maxcount, 1)) * nauxp * sizeof(double), "raw 3c block")))
     return rc;
   cudaMemsetAsync(raw.p, 0, raw.bytes, s);
-  cudaMemsetAsync(ctx->B.p, 0, static_cast<size_t>(naux) * ntile * TILE2 * sizeof(double), s);
+  cudaMemsetAsync(ctx->B.p, 0, static_cast<size_t>(nq) * ntile * TILE2 * sizeof(double), s);
   float ms = 0.f;
   for (long I0 = 0; I0 < nt; I0 += rows_per) {
     long I1 = std::min(nt, I0 + rows_per);
@@ -469,8 +483,9 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
       if (rc) { release(raw); return rc; }
     }
     cudaEventRecord(ctx->ev0, s);
-    launch_metric_contract_chunk(static_cast<const double*>(ctx->M.p), nauxp, static_cast<const double*>(raw.p),
-                                 layout, n, naux, nt, I0, I1, static_cast<double*>(ctx->B.p), s);
+    launch_metric_contract_chunk(static_cast<const double*>(ctx->M.p) + q0 * nauxp, nauxp, nauxp - q0,
+                                 static_cast<const double*>(raw.p), layout, n, nq, nt, I0, I1,
+                                 static_cast<double*>(ctx->B.p), s);
     cudaEventRecord(ctx->ev1, s);
     rc = cuda_check(ctx, cudaStreamSynchronize(s), "metric contraction");
     if (rc) { release(raw); return rc; }
@@ -486,7 +501,7 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
   ctx->stats.n = n;
   ctx->stats.npad = npad;
   ctx->stats.ntile = ntile;
-  ctx->stats.bytes_b = naux * ntile * TILE2 * static_cast<long>(sizeof(double));
+  ctx->stats.bytes_b = nq * ntile * TILE2 * static_cast<long>(sizeof(double));
   ctx->stats.bytes_b_mixed = 0;
   return RIJK_OK;
 }

@@ -51,6 +51,7 @@ struct rijk_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
 
   long n = 0, naux = 0, npad = 0, nt = 0, ntile = 0;
+  long q0 = 0, nq = 0;  // aux functions [q0, q0 + nq) held in B (all of them unless rijk_set_aux_range)
   int metric_form = RIJK_METRIC_INVSQRT;
   bool have_metric = false, have_b = false;
 
@@ -103,8 +104,9 @@ void launch_scan_nonfinite(const double* x, long count, int* err, cudaStream_t s
 
 // ---- k_metric.cu
 // B[Q][tile-packed e] = sum_P M[Q][P] * I3(pair(e), P) for the raw rows of tile rows [I0, I1).
-void launch_metric_contract_chunk(const double* M, long nauxp, const double* I3, int layout, long n, long naux,
-                                  long nt, long I0, long I1, double* B, cudaStream_t s);
+// M may start at a row offset q0 (mrows = rows left after it); B receives naux rows.
+void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const double* I3, int layout, long n,
+                                  long naux, long nt, long I0, long I1, double* B, cudaStream_t s);
 
 // ---- k_coulomb.cu
 int coulomb_nsplit(long tile_elems, long naux);

@@ -70,7 +70,7 @@ RIJK_API int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ) 
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_check(ctx, e, "rijk_coulomb_noalloc: cudaSetDevice");
 
-  const long n = ctx->n, naux = ctx->naux, nt = ctx->nt, npad = ctx->npad, ntile = ctx->ntile;
+  const long n = ctx->n, naux = ctx->nq, nt = ctx->nt, npad = ctx->npad, ntile = ctx->ntile;
   const long tile_elems = ntile * TILE2;
   const long nauxr = round_up(naux, 32);  // keeps the partial sums 256-byte aligned
   // scratch = [packed density weights | w | nsplit partial J tiles]

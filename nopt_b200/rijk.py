@@ -81,11 +81,13 @@ def lib():
         L.rijk_get_stats.argtypes = [_vp, P(Stats)]
         L.rijk_set_profiling.argtypes = [_vp, ctypes.c_int]
         L.rijk_set_metric.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_int]
+        L.rijk_set_aux_range.argtypes = [_vp, ctypes.c_long, ctypes.c_long]
         L.rijk_set_3c.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_int]
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
         L.rijk_grad.argtypes = [_vp, _dp, ctypes.c_long, _dp, ctypes.c_double, _dp, _dp, _dp, _dp]
+        L.rijk_mo_ints.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
         L.rijk_scf.argtypes = [_vp, _dp, _dp, ctypes.c_long, ctypes.c_double, P(ScfOpts), _dp, P(ScfResult)]
         L.rijk_fock_energy.argtypes = [_vp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, _dp]
         _LIB = L
@@ -147,6 +149,10 @@ class FockBuilder:
         self._check(lib().rijk_set_metric(self._h, _p(V), V.shape[0], form))
         self.naux = V.shape[0]
 
+    def set_aux_range(self, q0, q1):
+        """Hold only aux functions [q0, q1): Fock builds then return that slice's partial J, K."""
+        self._check(lib().rijk_set_aux_range(self._h, int(q0), int(q1)))
+
     def set_3c(self, I3, n, layout=LAYOUT_PACKED):
         I3 = _c(I3)
         self._check(lib().rijk_set_3c(self._h, _p(I3), int(n), I3.shape[-1], layout))
@@ -186,6 +192,18 @@ class FockBuilder:
         k = r.history_len
         out["history"] = [(r.history_energy[i], r.history_diis_err[i], r.history_mixed[i]) for i in range(k)]
         return r.energy, MO, out
+
+    def calc_2el_mo_ints_ri(self, DM_D, MO_VEC, MO_VEC1, MO_VEC2, n_c, n_a, t=0, want_jk=True):
+        """(MO_INTS (n_a^2 x n_a^2), J, K) as the reference's calc_2el_MO_INTS_RI (src/RI.cpp:178)."""
+        n = self.n
+        out = np.empty((n_a * n_a, n_a * n_a))
+        J = np.empty((n, n)) if want_jk else None
+        K = np.empty((n, n)) if want_jk else None
+        D = _c(DM_D) if want_jk else None
+        M0 = _c(MO_VEC) if (want_jk and n_c > 0) else None
+        self._check(lib().rijk_mo_ints(self._h, _p(D), _p(J), _p(K), _p(out), _p(M0), _p(_c(MO_VEC1)),
+                                       _p(_c(MO_VEC2)), int(n_c), int(n_a), int(t)))
+        return out, J, K
 
     def grad(self, MO, n_c, H, e_nuc, want_3c=False, want_metric=False):
         """(E, dE/dMO (n_c x n), dE/d(P|mu nu) packed [pair][P] or None, dE/d(P|Q) or None)."""

@@ -74,6 +74,24 @@ def dm_to_f_transform_ri(RI_AA, Vm05, DM, MO, n_c, n_ao):
     return J, K
 
 
+def calc_2el_mo_ints_ri(RI_AA, Vm05, n_ao, DM_D, MO_VEC, MO_VEC1, MO_VEC2, n_c, n_a, t=0):
+    """calc_2el_MO_INTS_RI (src/RI.cpp:178-292): active integrals MO_INTS (n_a^2 x n_a^2) in the
+    reference's (b a | d c) order, then the core J, K of DM_D / MO_VEC (None when DM_D is None)."""
+    naux = RI_AA.shape[1]
+    C1 = MO_VEC1.T if t else MO_VEC1                                  # n_a x n_ao
+    C2 = MO_VEC2.T if t else MO_VEC2
+    RI_aA = C1 @ RI_AA.reshape(n_ao, n_ao * naux)                     # :197-201  (a, nu, P)
+    RI_aA2 = RI_aA.reshape(n_a * n_ao, naux) @ Vm05                  # :203-207
+    T = RI_aA2.reshape(n_a, n_ao, naux).transpose(1, 0, 2)            # :209-215  (nu, a, Q)
+    RI_aa = C2 @ T.reshape(n_ao, n_a * naux)                          # :217-221  (b, a, Q)
+    R = RI_aa.reshape(n_a * n_a, naux)
+    MO_INTS = R @ R.T                                                 # :223-227
+    if DM_D is None:
+        return MO_INTS, None, None
+    J, K = dm_to_f_transform_ri(RI_AA, Vm05, DM_D, MO_VEC, n_c, n_ao)  # :235-287
+    return MO_INTS, J, K
+
+
 def gen_hf_dm(MO, n, n_el):
     """D[i,j] = sum_k MO[k,i] MO[k,j] over k < n_el (src/SCF.cpp:63-73)."""
     C = MO[:n_el]
