@@ -4,6 +4,9 @@
  * Drop-in for the reference's RI Fock-build routine and its set-up:
  *   rijk_set_metric   replaces RI_V_calc + S05_calc        src/libint_link.cpp:2049-2107, src/matr.cpp:372-401
  *   rijk_set_3c       replaces the RI_AA set-up of gen_RI_AA / regen_RI_AA
+ *   rijk_set_basis    replaces gen_RI_AA whole, integrals included  src/RI.cpp:34-79
+ *   rijk_eri2c        replaces RI_V_calc                            src/libint_link.cpp:2049-2107
+ *   rijk_eri3c        replaces calc_2el_AO_INTS_RI                  src/libint_link.cpp:2261-2350
  *                                                          src/RI.cpp:34-101 (consumer of calc_2el_AO_INTS_RI,
  *                                                          src/libint_link.cpp:2261-2350)
  *   rijk_fock         replaces DM_to_F_transform_RI        src/RI.cpp:115-176 (declared include/RI.h)
@@ -69,6 +72,8 @@ typedef struct {
   int profiled_stages;    /* number of valid entries of ms_stage (0 unless profiling is on)  */
   double ms_stage[12];    /* device time of each kernel of the last build, in launch order   */
   char stage_names[12][24];
+  double ms_setup_ints;   /* last rijk_set_basis: device time of the integral kernels          */
+  int kernels_setup_ints; /* integral kernels it launched                                    */
 } rijk_stats_t;
 
 int rijk_create(rijk_ctx** ctx, int device);
@@ -93,6 +98,34 @@ int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1);
 /* Three-centre integrals (host array, layout RIJK_LAYOUT_*).  Forms the fitted tensor
  * B^Q_{mu nu} = sum_P M_QP (P|mu nu) on the GPU, stored packed (mu >= nu) in HBM. */
 int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n_ao, long naux, int layout);
+
+/* A contracted Gaussian basis as shell arrays, in the order of a basis-set file.  Coefficients
+ * are as printed there; the library normalises them as libint does (x^l primitive
+ * normalisation, unit-norm contraction).  Spherical shells are real solid harmonics in the
+ * order m = -l .. l; Cartesian shells list x^a y^b z^c with a, then b, descending. */
+typedef struct {
+  int nshell;
+  const int* l;         /* angular momentum per shell, 0 .. 4                        */
+  const int* pure;      /* 1: spherical (2l+1 functions), 0: Cartesian               */
+  const int* nprim;     /* primitives per shell                                      */
+  const double* xyz;    /* shell centres in bohr, 3 per shell                        */
+  const double* exps;   /* primitive exponents, all shells concatenated              */
+  const double* coefs;  /* contraction coefficients, same order                      */
+} rijk_basis_t;
+
+/* (P|Q) of the aux basis computed on the GPU into a host naux x naux array. */
+int rijk_eri2c(rijk_ctx* ctx, const rijk_basis_t* aux, double* PQ);
+
+/* (mu nu|P) computed on the GPU into a host array in layout RIJK_LAYOUT_NOPT_FULL
+ * (n^2 naux doubles) or RIJK_LAYOUT_PACKED (n(n+1)/2 naux doubles). */
+int rijk_eri3c(rijk_ctx* ctx, const rijk_basis_t* orb, const rijk_basis_t* aux, int layout, double* I3);
+
+/* gen_RI_AA on the GPU: (P|Q), the metric factor (RIJK_METRIC_*), (mu nu|P) and the fitted
+ * tensor, with no integrals on the host and no host-to-device copy of them.  q1 > 0 keeps
+ * only the aux functions [q0, q1) (as rijk_set_aux_range); q1 = 0 keeps all of them.
+ * Equivalent to rijk_set_metric + rijk_set_aux_range + rijk_set_3c on the same integrals. */
+int rijk_set_basis(rijk_ctx* ctx, const rijk_basis_t* orb, const rijk_basis_t* aux, int metric_form, long q0,
+                   long q1);
 
 /* Drop-in for DM_to_F_transform_RI(J, K, DM, MO, n_c, n_ao): host pointers, synchronous. */
 int rijk_fock(rijk_ctx* ctx, const double* DM, const double* MO, long n_c, double* J, double* K, int precision);

@@ -28,6 +28,7 @@ CUDA_SOURCES = [
     "rijk/k_adjoint.cu",
     "rijk/k_moints.cu",
     "rijk/rijk_noalloc.cu",
+    "rijk/k_eri.cu",
 ]
 
 
@@ -66,7 +67,8 @@ def build_cuda(force=False, extra=()):
         for s in srcs:
             o = os.path.join(objdir, os.path.basename(s) + ".o")
             _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-                                  "-I" + INC, "-I" + os.path.join(CSRC, "rijk"), "--expt-relaxed-constexpr",
+                                  "-I" + INC, "-I" + os.path.join(CSRC, "rijk"), "-I" + os.path.join(CSRC, "host"),
+                                  "--expt-relaxed-constexpr",
                                   "-c", s, "-o", o] + list(extra))
             objs.append(o)
         _run([NVCC] + ARCH + ["-shared", "-o", out] + objs + ["-lcusolver", "-lcublas", "-lcudart"])

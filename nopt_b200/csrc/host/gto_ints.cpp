@@ -13,6 +13,7 @@
 // Normalisation follows libint: each primitive carries the x^l normalisation of its
 // exponent and the contraction is rescaled to unit norm.
 #include "gto_ints.h"
+#include "gto_tables.h"
 
 #include <omp.h>
 
@@ -25,51 +26,20 @@
 
 namespace {
 
-constexpr int LMAX = 4;                 // highest shell angular momentum supported (g)
-constexpr int NCART_MAX = (LMAX + 1) * (LMAX + 2) / 2;
-constexpr int LTOT = 3 * LMAX;          // highest Boys order in a three-centre integral
+using namespace gto_tab;
+
 constexpr int RD = LTOT + 1;            // edge of the R_{tuv} cube
-constexpr double PI = 3.14159265358979323846;
 
 int g_threads = 0;
 
-inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
-inline int cart_index(int l, int lx, int ly) { return (l - lx) * (l - lx + 1) / 2 + (l - lx - ly); }
-
-double dfact(int n) {  // (n)!! with (-1)!! = 0!! = 1
-  double r = 1.0;
-  for (int k = n; k > 1; k -= 2) r *= k;
-  return r;
-}
-
 // ---------------------------------------------------------------- Boys function ----
-// F_m(T) = int_0^1 t^{2m} exp(-T t^2) dt.  Tabulated on a grid from the convergent
-// series F_m(T) = exp(-T) sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)); evaluated by a
-// 7-term Taylor expansion about the nearest grid point (dF_m/dT = -F_{m+1}) followed by
-// downward recursion F_{m-1} = (2T F_m + exp(-T)) / (2m-1).  For T beyond the grid
-// F_0 = sqrt(pi/T)/2 (exp(-T) < 1e-17 there) and upward recursion is stable.
-constexpr double BOYS_TMAX = 40.0;
-constexpr int BOYS_NPER = 16;  // grid points per unit T
-constexpr int BOYS_NT = static_cast<int>(BOYS_TMAX) * BOYS_NPER + 1;
-constexpr int BOYS_MTAB = LTOT + 8;
+// Evaluated by a 7-term Taylor expansion about the nearest grid point of the table
+// (dF_m/dT = -F_{m+1}) followed by downward recursion F_{m-1} = (2T F_m + exp(-T)) / (2m-1).
+// For T beyond the grid F_0 = sqrt(pi/T)/2 (exp(-T) < 1e-17 there) and upward recursion is stable.
 std::vector<double> g_boys;  // [BOYS_NT][BOYS_MTAB]
 std::once_flag g_boys_once;
 
-void boys_table_init() {
-  g_boys.assign(static_cast<size_t>(BOYS_NT) * BOYS_MTAB, 0.0);
-  for (int i = 0; i < BOYS_NT; ++i) {
-    long double T = static_cast<long double>(i) / BOYS_NPER;
-    for (int m = 0; m < BOYS_MTAB; ++m) {
-      long double term = 1.0L / (2 * m + 1), sum = term;
-      for (int k = 1; k < 2000; ++k) {
-        term *= 2.0L * T / (2 * m + 2 * k + 1);
-        sum += term;
-        if (term < sum * 1e-21L) break;
-      }
-      g_boys[static_cast<size_t>(i) * BOYS_MTAB + m] = static_cast<double>(expl(-T) * sum);
-    }
-  }
-}
+void boys_table_init() { boys_table_fill(g_boys); }
 
 inline void boys(int mmax, double T, double* F) {
   if (T < BOYS_TMAX - 0.5 / BOYS_NPER) {
@@ -91,95 +61,6 @@ inline void boys(int mmax, double T, double* F) {
     F[0] = 0.5 * std::sqrt(PI / T);
     for (int m = 0; m < mmax; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2.0 * T);
   }
-}
-
-// ------------------------------------------------------- real solid harmonics ----
-// sph[l] is a (2l+1) x ncart(l) matrix C with  Y_m = sum_c C[m][c] phi_c, where phi_c
-// are the Cartesian functions normalised with the x^l convention.
-struct SphTables {
-  std::vector<double> c[LMAX + 1];
-  SphTables() {
-    std::vector<std::vector<double>> S[LMAX + 1];  // S[l][m+l] polynomial over cart(l)
-    S[0].assign(1, std::vector<double>(1, 1.0));
-    auto mulx = [](const std::vector<double>& p, int l, int dir) {  // p of degree l times x/y/z
-      std::vector<double> q(ncart(l + 1), 0.0);
-      for (int lx = l; lx >= 0; --lx)
-        for (int ly = l - lx; ly >= 0; --ly) {
-          int lz = l - lx - ly;
-          double v = p[cart_index(l, lx, ly)];
-          if (v == 0.0) continue;
-          int a = lx + (dir == 0), b = ly + (dir == 1);
-          (void)lz;
-          q[cart_index(l + 1, a, b)] += v;
-        }
-      return q;
-    };
-    auto mulr2 = [&](const std::vector<double>& p, int l) {
-      std::vector<double> x = mulx(mulx(p, l, 0), l + 1, 0);
-      std::vector<double> y = mulx(mulx(p, l, 1), l + 1, 1);
-      std::vector<double> z = mulx(mulx(p, l, 2), l + 1, 2);
-      for (size_t i = 0; i < x.size(); ++i) x[i] += y[i] + z[i];
-      return x;
-    };
-    for (int l = 0; l < LMAX; ++l) {
-      S[l + 1].assign(2 * l + 3, std::vector<double>());
-      double f = std::sqrt((l == 0 ? 2.0 : 1.0) * (2 * l + 1) / (2.0 * l + 2));
-      // S_{l+1,l+1} and S_{l+1,-(l+1)}
-      {
-        std::vector<double> a = mulx(S[l][2 * l], l, 0);  // x S_{l,l}
-        std::vector<double> b = mulx(S[l][2 * l], l, 1);  // y S_{l,l}
-        if (l > 0) {
-          std::vector<double> yb = mulx(S[l][0], l, 1);   // y S_{l,-l}
-          std::vector<double> xb = mulx(S[l][0], l, 0);   // x S_{l,-l}
-          for (size_t i = 0; i < a.size(); ++i) { a[i] -= yb[i]; b[i] += xb[i]; }
-        }
-        for (auto& v : a) v *= f;
-        for (auto& v : b) v *= f;
-        S[l + 1][2 * l + 2] = a;
-        S[l + 1][0] = b;
-      }
-      for (int m = -l; m <= l; ++m) {
-        std::vector<double> a = mulx(S[l][m + l], l, 2);
-        for (auto& v : a) v *= (2 * l + 1);
-        if (l >= 1 && std::abs(m) <= l - 1) {
-          std::vector<double> r = mulr2(S[l - 1][m + l - 1], l - 1);
-          double g = std::sqrt(static_cast<double>((l + m) * (l - m)));
-          for (size_t i = 0; i < a.size(); ++i) a[i] -= g * r[i];
-        }
-        double h = 1.0 / std::sqrt(static_cast<double>((l + m + 1) * (l - m + 1)));
-        for (auto& v : a) v *= h;
-        S[l + 1][m + l + 1] = a;
-      }
-    }
-    for (int l = 0; l <= LMAX; ++l) {
-      int nc = ncart(l);
-      c[l].assign(static_cast<size_t>(2 * l + 1) * nc, 0.0);
-      std::vector<int> cx(nc), cy(nc), cz(nc);
-      for (int lx = l; lx >= 0; --lx)
-        for (int ly = l - lx; ly >= 0; --ly) {
-          int i = cart_index(l, lx, ly);
-          cx[i] = lx; cy[i] = ly; cz[i] = l - lx - ly;
-        }
-      for (int m = 0; m < 2 * l + 1; ++m) {
-        const std::vector<double>& p = S[l][m];
-        double n2 = 0.0;  // <Y|Y> relative to <x^l|x^l>
-        for (int i = 0; i < nc; ++i)
-          for (int j = 0; j < nc; ++j) {
-            if (p[i] == 0.0 || p[j] == 0.0) continue;
-            int sx = cx[i] + cx[j], sy = cy[i] + cy[j], sz = cz[i] + cz[j];
-            if ((sx | sy | sz) & 1) continue;
-            n2 += p[i] * p[j] * dfact(sx - 1) * dfact(sy - 1) * dfact(sz - 1);
-          }
-        n2 /= dfact(2 * l - 1);
-        double s = 1.0 / std::sqrt(n2);
-        for (int i = 0; i < nc; ++i) c[l][static_cast<size_t>(m) * nc + i] = p[i] * s;
-      }
-    }
-  }
-};
-const SphTables& sph() {
-  static SphTables t;
-  return t;
 }
 
 struct CartList {
@@ -409,21 +290,7 @@ int gto_basis_create(gto_basis** out, int nshell, const int* l, const int* pure,
     for (int d = 0; d < 3; ++d) sh.xyz[d] = xyz[3 * s + d];
     sh.exps.assign(exps + po, exps + po + nprim[s]);
     sh.coefs.resize(nprim[s]);
-    const int L = sh.l;
-    for (int k = 0; k < sh.nprim; ++k) {
-      double a = sh.exps[k];
-      if (!(a > 0.0)) { delete b; return GTO_ERR_ARG; }
-      double n2 = std::pow(4.0 * a, L) * std::pow(2.0 * a / PI, 1.5) / dfact(2 * L - 1);
-      sh.coefs[k] = coefs[po + k] * std::sqrt(n2);
-    }
-    double norm = 0.0;  // <x^l|x^l> of the contraction
-    for (int i = 0; i < sh.nprim; ++i)
-      for (int j = 0; j < sh.nprim; ++j) {
-        double p = sh.exps[i] + sh.exps[j];
-        norm += sh.coefs[i] * sh.coefs[j] * dfact(2 * L - 1) / std::pow(2.0 * p, L) * std::pow(PI / p, 1.5);
-      }
-    double sc = 1.0 / std::sqrt(norm);
-    for (auto& c : sh.coefs) c *= sc;
+    if (!normalise_shell(sh.l, sh.nprim, sh.exps.data(), coefs + po, sh.coefs.data())) { delete b; return GTO_ERR_ARG; }
     sh.off = b->nbf;
     b->nbf += sh.nfunc;
     if (sh.l > b->lmax) b->lmax = sh.l;

@@ -256,7 +256,7 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DeviceBuf* bufs[] = {&ctx->M, &ctx->B, &ctx->Bmix, &ctx->stageD, &ctx->stageMO, &ctx->stageJ, &ctx->stageK,
-                       &ctx->Dt, &ctx->w, &ctx->Jpart, &ctx->MOp, &ctx->XT, &ctx->Kpart, &ctx->err, &ctx->scratch};
+                       &ctx->Dt, &ctx->w, &ctx->Jpart, &ctx->MOp, &ctx->XT, &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab};
   for (DeviceBuf* b : bufs) release(*b);
   if (ctx->cublas) cublasDestroy(ctx->cublas);
   if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
@@ -320,6 +320,11 @@ RIJK_API int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1) {
 
 RIJK_API int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int form) {
   if (!ctx) return RIJK_ERR_ARG;
+  return set_metric_impl(ctx, PQ, cudaMemcpyHostToDevice, naux, form);
+}
+
+namespace rijk {
+int set_metric_impl(rijk_ctx* ctx, const double* PQ, cudaMemcpyKind kind, long naux, int form) {
   if (!PQ || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_metric: null (P|Q) or naux <= 0");
   if (naux > 65535) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_metric: naux = %ld exceeds 65535", naux);
   if (form != RIJK_METRIC_INVSQRT && form != RIJK_METRIC_CHOLESKY)
@@ -344,7 +349,7 @@ RIJK_API int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int for
     return rc;
   }
   cudaEventRecord(ctx->ev0, s);
-  rc = cuda_check(ctx, cudaMemcpyAsync(V.p, PQ, naux * naux * sizeof(double), cudaMemcpyHostToDevice, s), "H2D (P|Q)");
+  rc = cuda_check(ctx, cudaMemcpyAsync(V.p, PQ, naux * naux * sizeof(double), kind, s), "copy (P|Q)");
   if (rc) { cleanup(); return rc; }
   cudaMemsetAsync(info.p, 0, 2 * sizeof(int), s);
   double* dV = static_cast<double*>(V.p);
@@ -424,10 +429,24 @@ RIJK_API int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int for
   if (hinfo[1] > 0) ctx->last_error = "warning: metric eigenvalues <= 0 dropped";
   return RIJK_OK;
 }
+}  // namespace rijk
 
 RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int layout) {
   if (!ctx) return RIJK_ERR_ARG;
   if (!I3 || n <= 0 || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_3c: null integrals or bad sizes");
+  cudaStream_t s = ctx->stream;
+  return set_3c_impl(ctx, n, naux, layout, [&](long, long, long first, long count, double* raw, long ld) {
+    if (count <= 0) return static_cast<int>(RIJK_OK);
+    return cuda_check(ctx,
+                      cudaMemcpy2DAsync(raw, ld * sizeof(double), I3 + first * naux, naux * sizeof(double),
+                                        naux * sizeof(double), static_cast<size_t>(count), cudaMemcpyHostToDevice, s),
+                      "H2D three-centre block");
+  });
+}
+
+namespace rijk {
+int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& fill) {
+  if (n <= 0 || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_3c: bad sizes");
   if (layout != RIJK_LAYOUT_NOPT_FULL && layout != RIJK_LAYOUT_PACKED)
     return set_err(ctx, RIJK_ERR_ARG, "rijk_set_3c: unknown layout %d", layout);
   if (!ctx->have_metric) return set_err(ctx, RIJK_ERR_STATE, "rijk_set_3c: call rijk_set_metric first");
@@ -444,7 +463,7 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
   release(ctx->Bmix);
   if ((rc = ensure(ctx, ctx->B, static_cast<size_t>(nq) * ntile * TILE2 * sizeof(double), "fitted tensor B")))
     return rc;
-  // Raw integrals go up in blocks of whole tile rows, at most ~2 GiB each.
+  // Raw integrals come in blocks of whole tile rows, at most ~2 GiB each.
   const double budget = 2.0 * 1024 * 1024 * 1024;
   long rows_per = std::max<long>(1, static_cast<long>(budget / (static_cast<double>(TILE) *
                                                                (layout == RIJK_LAYOUT_NOPT_FULL ? n : npad) * nauxp * 8.0)));
@@ -475,13 +494,8 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
     long I1 = std::min(nt, I0 + rows_per);
     long first, count;
     pairs_of(I0, I1, first, count);
-    if (count > 0) {
-      rc = cuda_check(ctx,
-                      cudaMemcpy2DAsync(raw.p, nauxp * sizeof(double), I3 + first * naux, naux * sizeof(double),
-                                        naux * sizeof(double), static_cast<size_t>(count), cudaMemcpyHostToDevice, s),
-                      "H2D three-centre block");
-      if (rc) { release(raw); return rc; }
-    }
+    rc = fill(I0 * TILE, std::min(I1 * TILE, n), first, count, static_cast<double*>(raw.p), nauxp);
+    if (rc) { release(raw); return rc; }
     cudaEventRecord(ctx->ev0, s);
     launch_metric_contract_chunk(static_cast<const double*>(ctx->M.p) + q0 * nauxp, nauxp, nauxp - q0,
                                  static_cast<const double*>(raw.p), layout, n, nq, nt, I0, I1,
@@ -505,6 +519,7 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
   ctx->stats.bytes_b_mixed = 0;
   return RIJK_OK;
 }
+}  // namespace rijk
 
 namespace rijk {
 // Reads and clears the device error word the kernels raise instead of trapping.

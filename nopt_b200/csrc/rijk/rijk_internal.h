@@ -19,6 +19,7 @@
 #include <cusolverDn.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 
 #include "rijk.h"
@@ -68,6 +69,7 @@ struct rijk_ctx {
   rijk::DeviceBuf Kpart;  // exchange split-K partials
   rijk::DeviceBuf err;    // int device error word
   rijk::DeviceBuf scratch;  // misc small
+  rijk::DeviceBuf eri_tab;  // integral tables (Boys grid, harmonics, aux term lists)
 
   rijk_stats_t stats{};
   std::string last_error;
@@ -95,6 +97,14 @@ int check_fock_args(rijk_ctx* ctx, long nocc, int precision);
 // One Fock build on device pointers (J into dJ, K into dK), asynchronous on ctx->stream.
 int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
                      int precision);
+// Metric factor from (P|Q) held in host memory (cudaMemcpyHostToDevice) or device memory.
+int set_metric_impl(rijk_ctx* ctx, const double* PQ, cudaMemcpyKind kind, long naux, int form);
+// Fitted tensor from three-centre integrals that `fill` writes, one block of tile rows at a time:
+// fill(mu0, mu1, first, count, raw, ld) writes the `count` pair rows of functions mu in
+// [mu0, mu1) (pair-row index minus `first`, in `layout`) with row pitch ld (>= naux, zero past
+// naux) into the device buffer raw.
+using ChunkFill = std::function<int(long mu0, long mu1, long first, long count, double* raw, long ld)>;
+int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& fill);
 
 // ---- k_pack.cu
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);

@@ -76,6 +76,8 @@ class Basis:
         self._h = h
         self.nbf = lib().gto_basis_nbf(h)
         self.pure = pure
+        # shell arrays as handed to the library (also the rijk_basis_t of the GPU integrals)
+        self.arrays = (l, pu, npr, xyz, ex, co)
 
     @classmethod
     def for_molecule(cls, name, mol, pure=True):

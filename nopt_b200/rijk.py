@@ -4,6 +4,8 @@ The methods mirror the reference's RI interface (include/RI.h of the reference):
 
   FockBuilder.set_metric          RI_V_calc + S05_calc        src/libint_link.cpp:2049, src/matr.cpp:372
   FockBuilder.set_3c              RI_AA set-up of gen_RI_AA   src/RI.cpp:34-79
+  FockBuilder.set_basis           gen_RI_AA with the integrals computed on the GPU
+  FockBuilder.eri2c / eri3c       RI_V_calc / calc_2el_AO_INTS_RI   src/libint_link.cpp:2049-2107, :2261-2350
   FockBuilder.dm_to_f_transform_ri  DM_to_F_transform_RI      src/RI.cpp:115-176
   FockBuilder.calc_f_ao           F and E of calc_F_AO / RHF  src/molecule.cpp:4407-4438, src/SCF.cpp:134
 
@@ -36,7 +38,22 @@ class Stats(ctypes.Structure):
                 ("npad", ctypes.c_long), ("ntile", ctypes.c_long), ("bytes_b", ctypes.c_long),
                 ("bytes_b_mixed", ctypes.c_long), ("kernels_last_fock", ctypes.c_int),
                 ("profiled_stages", ctypes.c_int), ("ms_stage", ctypes.c_double * 12),
-                ("stage_names", (ctypes.c_char * 24) * 12)]
+                ("stage_names", (ctypes.c_char * 24) * 12), ("ms_setup_ints", ctypes.c_double),
+                ("kernels_setup_ints", ctypes.c_int)]
+
+
+class BasisT(ctypes.Structure):
+    """rijk_basis_t: a contracted basis as shell arrays."""
+    _fields_ = [("nshell", ctypes.c_int), ("l", ctypes.POINTER(ctypes.c_int)), ("pure", ctypes.POINTER(ctypes.c_int)),
+                ("nprim", ctypes.POINTER(ctypes.c_int)), ("xyz", _dp), ("exps", _dp), ("coefs", _dp)]
+
+
+def basis_t(basis):
+    """rijk_basis_t over the shell arrays of an nopt_b200.ints.Basis (kept alive by the Basis)."""
+    l, pu, npr, xyz, ex, co = basis.arrays
+    ip = ctypes.POINTER(ctypes.c_int)
+    return BasisT(len(l), l.ctypes.data_as(ip), pu.ctypes.data_as(ip), npr.ctypes.data_as(ip),
+                  xyz.ctypes.data_as(_dp), ex.ctypes.data_as(_dp), co.ctypes.data_as(_dp))
 
 
 class ScfOpts(ctypes.Structure):
@@ -83,6 +100,9 @@ def lib():
         L.rijk_set_metric.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_int]
         L.rijk_set_aux_range.argtypes = [_vp, ctypes.c_long, ctypes.c_long]
         L.rijk_set_3c.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_int]
+        L.rijk_eri2c.argtypes = [_vp, P(BasisT), _dp]
+        L.rijk_eri3c.argtypes = [_vp, P(BasisT), P(BasisT), ctypes.c_int, _dp]
+        L.rijk_set_basis.argtypes = [_vp, P(BasisT), P(BasisT), ctypes.c_int, ctypes.c_long, ctypes.c_long]
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
@@ -157,6 +177,28 @@ class FockBuilder:
         I3 = _c(I3)
         self._check(lib().rijk_set_3c(self._h, _p(I3), int(n), I3.shape[-1], layout))
         self.n = n
+
+    def set_basis(self, orb, aux, metric_form=METRIC_INVSQRT, q0=0, q1=0):
+        """gen_RI_AA on the GPU: integrals, metric factor and fitted tensor from two Basis objects."""
+        bo, ba = basis_t(orb), basis_t(aux)
+        self._check(lib().rijk_set_basis(self._h, ctypes.byref(bo), ctypes.byref(ba), metric_form, int(q0), int(q1)))
+        self.n = orb.nbf
+
+    def eri2c(self, aux):
+        """(P|Q) computed on the GPU (naux x naux)."""
+        ba = basis_t(aux)
+        V = np.empty((aux.nbf, aux.nbf))
+        self._check(lib().rijk_eri2c(self._h, ctypes.byref(ba), _p(V)))
+        return V
+
+    def eri3c(self, orb, aux, layout=LAYOUT_PACKED):
+        """(mu nu|P) computed on the GPU, in LAYOUT_PACKED ([pair][P]) or LAYOUT_NOPT_FULL ([mu][nu][P])."""
+        bo, ba = basis_t(orb), basis_t(aux)
+        n, naux = orb.nbf, aux.nbf
+        shape = (n * (n + 1) // 2, naux) if layout == LAYOUT_PACKED else (n, n, naux)
+        out = np.empty(shape)
+        self._check(lib().rijk_eri3c(self._h, ctypes.byref(bo), ctypes.byref(ba), layout, _p(out)))
+        return out
 
     def dm_to_f_transform_ri(self, DM, MO, n_c, precision=PREC_FP64, J=None, K=None):
         """(J, K) exactly as the reference's DM_to_F_transform_RI(J, K, DM, MO, n_c, n_ao)."""
