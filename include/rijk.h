@@ -4,11 +4,14 @@
  * Drop-in for the reference's RI Fock-build routine and its set-up:
  *   rijk_set_metric   replaces RI_V_calc + S05_calc        src/libint_link.cpp:2049-2107, src/matr.cpp:372-401
  *   rijk_set_3c       replaces the RI_AA set-up of gen_RI_AA / regen_RI_AA
+ *                                                          src/RI.cpp:34-101 (consumer of calc_2el_AO_INTS_RI,
+ *                                                          src/libint_link.cpp:2261-2350)
  *   rijk_set_basis    replaces gen_RI_AA whole, integrals included  src/RI.cpp:34-79
  *   rijk_eri2c        replaces RI_V_calc                            src/libint_link.cpp:2049-2107
  *   rijk_eri3c        replaces calc_2el_AO_INTS_RI                  src/libint_link.cpp:2261-2350
- *                                                          src/RI.cpp:34-101 (consumer of calc_2el_AO_INTS_RI,
- *                                                          src/libint_link.cpp:2261-2350)
+ *   rijk_mo_calc      replaces RI_data::MO_calc                     src/RI.cpp:469-587
+ *   rijk_mo_ints_aaag replaces calc_2el_MO_INTS_AAAG_RI             src/RI.cpp:294-346
+ *   rijk_soscf_hess_ints replaces calc_SOSCF_hess_INTS_RI           src/RI.cpp:348-450
  *   rijk_fock         replaces DM_to_F_transform_RI        src/RI.cpp:115-176 (declared include/RI.h)
  *                     and the J/K tail of calc_2el_MO_INTS_RI  src/RI.cpp:235-287
  *   rijk_fock_energy  F = H + (2J - K) c and the RHF energy   src/molecule.cpp:4407-4438, src/SCF.cpp:134
@@ -212,6 +215,31 @@ int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long n_c, double e
  * of MO_VEC (as rijk_fock).  Host pointers; synchronous; FP64. */
 int rijk_mo_ints(rijk_ctx* ctx, const double* DM_D, double* J, double* K, double* MO_INTS, const double* MO_VEC,
                  const double* MO_VEC1, const double* MO_VEC2, long n_c, long n_a, long t);
+
+/* ---- MO-basis fitted tensors (post-SCF: CASSCF, perturbation theory) ----
+ * (p a|Q) below is sum_{mu nu} C1[p][mu] C2[a][nu] B^Q_{mu nu}.  With RIJK_METRIC_INVSQRT it is the
+ * reference's tensor; with the Cholesky form it differs by an orthogonal rotation of Q, and
+ * every contraction over Q is the same.  Orbitals are rows of n_ao coefficients. */
+
+/* out[(p*n2 + a)*naux + Q] for the rows of C1 (n1 x n_ao) and C2 (n2 x n_ao). */
+int rijk_mo_tensor(rijk_ctx* ctx, const double* C1, long n1, const double* C2, long n2, double* out);
+
+/* RI_data::MO_calc (src/RI.cpp:469-587): VEC holds n_cor core, n_act active and n_vac virtual
+ * rows.  CC[(i n_cor + j)], VC[(v n_cor + j)], AA[(t n_act + u)], CA[(i n_act + u)] and
+ * VA[(v n_act + u)], each times naux; any output may be NULL. */
+int rijk_mo_calc(rijk_ctx* ctx, const double* VEC, long n_cor, long n_act, long n_vac, double* CC, double* VC,
+                 double* AA, double* CA, double* VA);
+
+/* calc_2el_MO_INTS_AAAG_RI (src/RI.cpp:294-346): MO_INTS[((t n_a + u) n_a + v) n_mo + x] = (tu|vx)
+ * for active t, u, v (rows n_c .. n_c+n_a-1 of MO_VEC) and all n_mo rows x (the reference uses
+ * n_mo = n_ao). */
+int rijk_mo_ints_aaag(rijk_ctx* ctx, double* MO_INTS, const double* MO_VEC, long n_c, long n_a, long n_mo);
+
+/* calc_SOSCF_hess_INTS_RI (src/RI.cpp:348-450): aa_J[(p n_a + t) n_a + u] = (pp|tu) and
+ * aa_K[(p n_a + t) n_a + u] = (pt|pu) for all n_mo orbital rows p.  (The reference's cv_J / cv_K
+ * arguments are never written by it and have no counterpart here.) */
+int rijk_soscf_hess_ints(rijk_ctx* ctx, double* aa_J, double* aa_K, const double* MO_VEC, long n_c, long n_a,
+                         long n_mo);
 
 /* Adjoint of the Fock build (no reference counterpart; the reference differentiates by finite
  * differences, src/QM_calc.cpp:142).  For the orbitals MO (n_c rows of n, host) and D = C^T C:

@@ -29,6 +29,7 @@ CUDA_SOURCES = [
     "rijk/k_moints.cu",
     "rijk/rijk_noalloc.cu",
     "rijk/k_eri.cu",
+    "rijk/k_mo_ri.cu",
 ]
 
 

@@ -103,6 +103,10 @@ def lib():
         L.rijk_eri2c.argtypes = [_vp, P(BasisT), _dp]
         L.rijk_eri3c.argtypes = [_vp, P(BasisT), P(BasisT), ctypes.c_int, _dp]
         L.rijk_set_basis.argtypes = [_vp, P(BasisT), P(BasisT), ctypes.c_int, ctypes.c_long, ctypes.c_long]
+        L.rijk_mo_tensor.argtypes = [_vp, _dp, ctypes.c_long, _dp, ctypes.c_long, _dp]
+        L.rijk_mo_calc.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long, _dp, _dp, _dp, _dp, _dp]
+        L.rijk_mo_ints_aaag.argtypes = [_vp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
+        L.rijk_soscf_hess_ints.argtypes = [_vp, _dp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
@@ -131,6 +135,7 @@ class FockBuilder:
         if rc != OK:
             raise RijkError(rc, "rijk_create(device=%d) failed" % device)
         self._h = h
+        self._q = None  # aux slice (q0, q1) held, None for all
         self.n = self.naux = None
 
     def close(self):
@@ -168,10 +173,12 @@ class FockBuilder:
         V = _c(V)
         self._check(lib().rijk_set_metric(self._h, _p(V), V.shape[0], form))
         self.naux = V.shape[0]
+        self._q = None
 
     def set_aux_range(self, q0, q1):
         """Hold only aux functions [q0, q1): Fock builds then return that slice's partial J, K."""
         self._check(lib().rijk_set_aux_range(self._h, int(q0), int(q1)))
+        self._q = (int(q0), int(q1))
 
     def set_3c(self, I3, n, layout=LAYOUT_PACKED):
         I3 = _c(I3)
@@ -182,6 +189,7 @@ class FockBuilder:
         """gen_RI_AA on the GPU: integrals, metric factor and fitted tensor from two Basis objects."""
         bo, ba = basis_t(orb), basis_t(aux)
         self._check(lib().rijk_set_basis(self._h, ctypes.byref(bo), ctypes.byref(ba), metric_form, int(q0), int(q1)))
+        self._q = (int(q0), int(q1)) if q1 > 0 else None
         self.n = orb.nbf
 
     def eri2c(self, aux):
@@ -199,6 +207,45 @@ class FockBuilder:
         out = np.empty(shape)
         self._check(lib().rijk_eri3c(self._h, ctypes.byref(bo), ctypes.byref(ba), layout, _p(out)))
         return out
+
+    def mo_tensor(self, C1, C2):
+        """(p a|Q) for the orbital rows of C1 and C2, shape (n1 * n2, naux)."""
+        C1, C2 = _c(C1), _c(C2)
+        out = np.empty((C1.shape[0] * C2.shape[0], self._naux()))
+        self._check(lib().rijk_mo_tensor(self._h, _p(C1), C1.shape[0], _p(C2), C2.shape[0], _p(out)))
+        return out
+
+    def mo_calc(self, VEC, n_cor, n_act, n_vac):
+        """RI_data::MO_calc: dict of the CC, VC, AA, CA, VA tensors ((p n2 + a), Q)."""
+        VEC = _c(VEC)
+        na = self._naux()
+        shapes = {"CC": n_cor * n_cor, "VC": n_vac * n_cor, "AA": n_act * n_act, "CA": n_cor * n_act,
+                  "VA": n_vac * n_act}
+        out = {k: np.empty((v, na)) for k, v in shapes.items()}
+        self._check(lib().rijk_mo_calc(self._h, _p(VEC), n_cor, n_act, n_vac, *[_p(out[k]) for k in
+                                                                                    ("CC", "VC", "AA", "CA", "VA")]))
+        return out
+
+    def mo_ints_aaag(self, MO_VEC, n_c, n_a, n_mo=None):
+        """calc_2el_MO_INTS_AAAG_RI: (tu|vx) as an (n_a^3, n_mo) array."""
+        MO_VEC = _c(MO_VEC)
+        n_mo = MO_VEC.shape[0] if n_mo is None else n_mo
+        out = np.empty((n_a ** 3, n_mo))
+        self._check(lib().rijk_mo_ints_aaag(self._h, _p(out), _p(MO_VEC), n_c, n_a, n_mo))
+        return out
+
+    def soscf_hess_ints(self, MO_VEC, n_c, n_a, n_mo=None):
+        """calc_SOSCF_hess_INTS_RI: (aa_J, aa_K), each (n_mo, n_a^2)."""
+        MO_VEC = _c(MO_VEC)
+        n_mo = MO_VEC.shape[0] if n_mo is None else n_mo
+        aJ, aK = np.empty((n_mo, n_a * n_a)), np.empty((n_mo, n_a * n_a))
+        self._check(lib().rijk_soscf_hess_ints(self._h, _p(aJ), _p(aK), _p(MO_VEC), n_c, n_a, n_mo))
+        return aJ, aK
+
+    def _naux(self):
+        s = Stats()
+        self._check(lib().rijk_get_stats(self._h, ctypes.byref(s)))
+        return s.naux if self._q is None else self._q[1] - self._q[0]
 
     def dm_to_f_transform_ri(self, DM, MO, n_c, precision=PREC_FP64, J=None, K=None):
         """(J, K) exactly as the reference's DM_to_F_transform_RI(J, K, DM, MO, n_c, n_ao)."""

@@ -8,6 +8,8 @@ algorithm for the hot path in the reference's own operation order:
 
   * DM_to_F_transform_RI          src/RI.cpp:115-176
   * CASSCF inactive J/K tail      src/RI.cpp:235-287 (same algorithm, D_core / C_core)
+  * MO-basis tensors: calc_2el_MO_INTS_RI src/RI.cpp:178-292, calc_2el_MO_INTS_AAAG_RI :294-346,
+    calc_SOSCF_hess_INTS_RI :348-450, RI_data::MO_calc :469-587
   * S05_calc  (metric V^-1/2)     src/matr.cpp:372-401
   * gen_HF_DM (D = sum_i C_i C_i^T, normalised to 1)   src/SCF.cpp:63-73
   * calc_F_AO (F = H + (2J - K) c, mc = 0/1/2)        src/molecule.cpp:4407-4438
@@ -90,6 +92,58 @@ def calc_2el_mo_ints_ri(RI_AA, Vm05, n_ao, DM_D, MO_VEC, MO_VEC1, MO_VEC2, n_c, 
         return MO_INTS, None, None
     J, K = dm_to_f_transform_ri(RI_AA, Vm05, DM_D, MO_VEC, n_c, n_ao)  # :235-287
     return MO_INTS, J, K
+
+
+def _half(RI_AA, Vm05, C, n_ao):
+    """(tA|K) -> the reference's transposed (A t|K) buffer: T[b][(a, k)] = sum_mu C[a,mu] (mu b|P) Vm05[P,k]
+    (the dgemm pair and OpenMP transpose repeated at src/RI.cpp:305-323, :361-379, :480-498)."""
+    naux = RI_AA.shape[1]
+    na = C.shape[0]
+    RI_aA = C @ RI_AA.reshape(n_ao, n_ao * naux)
+    RI_aA2 = RI_aA.reshape(na * n_ao, naux) @ Vm05
+    T = RI_aA2.reshape(na, n_ao, naux).transpose(1, 0, 2).reshape(n_ao, na * naux)
+    return RI_aA2, T
+
+
+def mo_calc(RI_AA, Vm05, VEC, n_cor, n_act, n_vac, n_ao):
+    """RI_data::MO_calc (src/RI.cpp:469-587): the CC, VC, AA, CA, VA tensors, each [(p n2 + a)][k]."""
+    naux = RI_AA.shape[1]
+    COR, ACT = VEC[:n_cor], VEC[n_cor:n_cor + n_act]
+    VAC = VEC[n_cor + n_act:n_cor + n_act + n_vac]
+    _, T = _half(RI_AA, Vm05, COR, n_ao)                              # :480-498
+    CC = (COR @ T).reshape(n_cor * n_cor, naux)                       # :500-506
+    VC = (VAC @ T).reshape(n_vac * n_cor, naux)                       # :508-514
+    _, T = _half(RI_AA, Vm05, ACT, n_ao)                              # :521-539
+    AA = (ACT @ T).reshape(n_act * n_act, naux)                       # :541-547
+    CA = (COR @ T).reshape(n_cor * n_act, naux)                       # :548-554
+    VA = (VAC @ T).reshape(n_vac * n_act, naux)                       # :555-561
+    return CC, VC, AA, CA, VA
+
+
+def mo_ints_aaag(RI_AA, Vm05, MO_VEC, n_c, n_a, n_ao):
+    """calc_2el_MO_INTS_AAAG_RI (src/RI.cpp:294-346): MO_INTS[(t u v)][x] = (tu|vx), x < n_ao."""
+    naux = RI_AA.shape[1]
+    CA = MO_VEC[n_c:n_c + n_a]
+    RI_aA2, T = _half(RI_AA, Vm05, CA, n_ao)                          # :305-323
+    RI_aa = (CA @ T).reshape(n_a * n_a, naux)                         # :325-330
+    aaag2 = RI_aa @ RI_aA2.T                                          # :332-337  (tu | v A)
+    return aaag2.reshape(n_a ** 3, n_ao) @ MO_VEC[:n_ao].T            # :338-343
+
+
+def soscf_hess_ints(RI_AA, Vm05, MO_VEC, n_c, n_a, n_ao):
+    """calc_SOSCF_hess_INTS_RI (src/RI.cpp:348-450): aa_J[p][(t u)] = (pp|tu), aa_K[p][(t u)] = (pt|pu)."""
+    naux = RI_AA.shape[1]
+    C = MO_VEC[:n_ao]
+    CA = MO_VEC[n_c:n_c + n_a]
+    _, T = _half(RI_AA, Vm05, CA, n_ao)                               # :361-379
+    RI_aa = (CA @ T).reshape(n_a * n_a, naux)                         # :381-386
+    TMP = np.einsum("pi,pj->pij", C, C).reshape(n_ao, n_ao * n_ao)    # :389-393
+    RI_pp = TMP @ RI_AA                                               # :394-399
+    RI_pp_2 = RI_pp @ Vm05.T                                          # :404-407
+    aa_J = RI_pp_2 @ RI_aa.T                                          # :410-413
+    RI_aA2 = (C @ T).reshape(n_ao, n_a, naux)                         # :416-421  (p, a, k)
+    aa_K = np.einsum("pik,pjk->pij", RI_aA2, RI_aA2).reshape(n_ao, n_a * n_a)  # :423-428
+    return aa_J, aa_K
 
 
 def gen_hf_dm(MO, n, n_el):
