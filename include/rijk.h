@@ -177,12 +177,23 @@ typedef struct {
   const double* guess_dm;
   const double* guess_rows;
   long guess_nrows;
+  /* The converger (appended fields; zero = defaults). */
+  int converger;          /* RIJK_CONV_DIIS (default) or RIJK_CONV_SOSCF, the reference's RHF step:
+                             L-BFGS on the occupied-virtual rotations with the diagonal Hessian
+                             4 (e_a - e_i), rotation I + X - X^T orthonormalised by Gram-Schmidt
+                             (src/SCF.cpp:125-174, src/converger_2_1.cpp:55-125, src/l-bfgs_2_1.cpp) */
+  double conv_grad;       /* SOSCF: converged when max |4 F_ai| < conv_grad; default 1e-7          */
+  double conv_energy;     /* SOSCF: or when |E - E_previous| < conv_energy; default 1e-10          */
+  int lbfgs_vectors;      /* SOSCF: curvature pairs kept, 1 .. 32; default min(n_mo, 20, max_iter)  */
 } rijk_scf_opts_t;
+
+#define RIJK_CONV_DIIS 0
+#define RIJK_CONV_SOSCF 1
 
 typedef struct {
   double energy;          /* E = tr(F D) + tr(H D) + e_nuc of the converged FP64 Fock build     */
   double dm_rms;          /* last RMS density change                                          */
-  double diis_err;        /* last max |X^T (F D S - S D F) X|                                  */
+  double diis_err;        /* last max |X^T (F D S - S D F) X|; with SOSCF, the last max |4 F_ai| */
   int iterations;         /* Fock builds, the final FP64 one included                          */
   int iterations_mixed;   /* of which in the mixed form                                        */
   int converged;
@@ -194,15 +205,16 @@ typedef struct {
   double ms_diag_phase;   /* wall time of diagonalisation + new density                        */
   int history_len;        /* entries of the per-iteration trace below (first 128 iterations)   */
   double history_energy[128];
-  double history_diis_err[128];
+  double history_diis_err[128];  /* per build: the DIIS error, or max |4 F_ai| with SOSCF          */
   int history_mixed[128]; /* 1 where the iteration used the mixed form                          */
 } rijk_scf_result_t;
 
-/* Restricted Hartree-Fock on the GPU around the Fock build: the role of the reference's RHF
- * loop (src/SCF.cpp:78-223), with DIIS on F D S - S D F in place of its SOSCF/L-BFGS step (the
- * converged energy is the same).  H and S are n x n host arrays; n_c occupied orbitals; the
- * core-Hamiltonian guess starts it.  Diagonalisation, DIIS extrapolation and the energy are
- * FP64 on the device.  MO (optional, n x n host) receives the orbitals, one per row, as the
+/* Restricted Hartree-Fock on the GPU around the Fock build: the reference's RHF loop
+ * (src/SCF.cpp:78-223).  The converger is Pulay DIIS on F D S - S D F (default) or, with
+ * opts->converger = RIJK_CONV_SOSCF, the reference's own SOSCF/L-BFGS orbital-rotation step and
+ * convergence test (max |4 F_ai| or |dE|); both reach the same energy.  H and S are n x n host
+ * arrays; n_c occupied orbitals; the core-Hamiltonian guess (or opts' guess) starts it.
+ * Diagonalisation, the converger's algebra and the energy are FP64 on the device.  MO (optional, n x n host) receives the orbitals, one per row, as the
  * reference's MO_VEC; E as in src/SCF.cpp:134. */
 int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long n_c, double e_nuc, const rijk_scf_opts_t* opts,
              double* MO, rijk_scf_result_t* result);

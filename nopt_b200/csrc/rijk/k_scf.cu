@@ -2,9 +2,15 @@
 //
 // The reference's RHF loop (src/SCF.cpp:78-223) builds D = sum_i C_i C_i^T (src/SCF.cpp:63-73),
 // calls the RI Fock build, forms F = H + 2J - K and E = tr(F D) + tr(H D) + V_nuc
-// (src/SCF.cpp:134) and takes an SOSCF/L-BFGS step.  Here the step is Pulay DIIS on the
-// commutator F D S - S D F in the orthogonal basis X = S^-1/2 (canonical, eigenvalues of S
-// below `lindep` dropped), with diagonalisation of X^T F X; the converged energy is the same.
+// (src/SCF.cpp:134) and takes an SOSCF/L-BFGS step.  Two convergers run here: Pulay DIIS on
+// the commutator F D S - S D F in the orthogonal basis X = S^-1/2 (canonical, eigenvalues of S
+// below `lindep` dropped), with diagonalisation of X^T F X; and the reference's SOSCF step
+// (src/converger_2_1.cpp:55-125 with the L-BFGS of src/l-bfgs_2_1.cpp, built with
+// LBFGS_RETURN_STEP): gradient g_ia = 4 F_ai and diagonal Hessian 4 (F_aa - F_ii) in the MO
+// basis, a two-loop L-BFGS step capped at 0.1 per angle, the rotation I + X - X^T made
+// orthonormal row by row (Gram-Schmidt, here as a QR factorisation with R's diagonal made
+// positive, which gives the same rows) and applied to the orbitals.  The L-BFGS inner products
+// stay on the device: each coefficient is read by the kernel that applies it.
 // Everything n x n stays on the device in FP64: the small products are cuBLAS DGEMMs, the
 // eigenproblems cuSOLVER syevd, the inner products deterministic two-stage reductions; only
 // the DIIS coefficients ((m+1) x (m+1) system) are solved on the host.
@@ -17,6 +23,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "dmma.cuh"
@@ -133,6 +140,83 @@ __global__ void k_axpy_set(double c, const double* __restrict__ x, long n, doubl
   for (; idx < n; idx += static_cast<long>(gridDim.x) * blockDim.x) y[idx] = first ? c * x[idx] : y[idx] + c * x[idx];
 }
 
+// ---- SOSCF (src/converger_2_1.cpp:55-125)
+// g[i nv + a] = 4 F_MO[nocc + a][i], h[i nv + a] = 4 (F_MO[nocc + a][nocc + a] - F_MO[i][i])
+__global__ void k_soscf_grad(const double* __restrict__ Fmo, long nm, long nocc, double* __restrict__ g,
+                             double* __restrict__ h) {
+  const long nv = nm - nocc;
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < nocc * nv;
+       idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    const long i = idx / nv, a = nocc + idx % nv;
+    g[idx] = 4.0 * Fmo[a + i * nm];
+    h[idx] = 4.0 * (Fmo[a * (nm + 1)] - Fmo[i * (nm + 1)]);
+  }
+}
+
+__global__ void k_sub(const double* __restrict__ a, const double* __restrict__ b, long n, double* __restrict__ out) {
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < n;
+       idx += static_cast<long>(gridDim.x) * blockDim.x)
+    out[idx] = a[idx] - b[idx];
+}
+
+// y += (ca dev[sa] + cb dev[sb]) x, a slot < 0 contributing nothing: the L-BFGS updates with
+// their inner products taken from device memory.
+__global__ void k_axpy_dev(double* __restrict__ y, const double* __restrict__ x, long n, const double* __restrict__ dev,
+                           int sa, double ca, int sb, double cb) {
+  const double c = (sa >= 0 ? ca * dev[sa] : 0.0) + (sb >= 0 ? cb * dev[sb] : 0.0);
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < n;
+       idx += static_cast<long>(gridDim.x) * blockDim.x)
+    y[idx] += c * x[idx];
+}
+
+__global__ void k_div(const double* __restrict__ q, const double* __restrict__ h, long n, double* __restrict__ s) {
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < n;
+       idx += static_cast<long>(gridDim.x) * blockDim.x)
+    s[idx] = q[idx] / h[idx];
+}
+
+// x = s zoom and x2 = s zoom, zoom = -min(1, xmax / max|s|) with max|s| at dev[smax]
+// (src/l-bfgs_2_1.cpp:96-110, :118-121); the zoom is also stored at dev[szoom].
+__global__ void k_zoom(const double* __restrict__ s, long n, double* __restrict__ dev, int smax, int szoom, double xmax,
+                       double* __restrict__ x, double* __restrict__ x2) {
+  const double m = dev[smax];
+  const double zoom = (m > xmax) ? -xmax / m : -1.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) dev[szoom] = zoom;
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < n;
+       idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    const double v = s[idx] * zoom;
+    x[idx] = v;
+    x2[idx] = v;
+  }
+}
+
+// R[p][q] (row-major, nm x nm) = delta_pq + X_pq - X_qp with X[i][nocc + a] = x[i nv + a]
+// (src/converger_2_1.cpp:107-113)
+__global__ void k_rot_build(const double* __restrict__ x, long nm, long nocc, double* __restrict__ R) {
+  const long nv = nm - nocc;
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < nm * nm;
+       idx += static_cast<long>(gridDim.x) * blockDim.x) {
+    const long p = idx / nm, q = idx % nm;
+    double v = p == q ? 1.0 : 0.0;
+    if (p < nocc && q >= nocc) v = x[p * nv + (q - nocc)];
+    if (q < nocc && p >= nocc) v = -x[q * nv + (p - nocc)];
+    R[idx] = v;
+  }
+}
+
+__global__ void k_copy_diag(const double* __restrict__ A, long nm, double* __restrict__ d) {
+  for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < nm;
+       i += static_cast<long>(gridDim.x) * blockDim.x)
+    d[i] = A[i * (nm + 1)];
+}
+
+// column j of Q (column-major nm x nm) times sign(d[j]): the QR factor with R's diagonal positive
+__global__ void k_sign_cols(double* __restrict__ Q, long nm, const double* __restrict__ d) {
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < nm * nm;
+       idx += static_cast<long>(gridDim.x) * blockDim.x)
+    if (d[idx / nm] < 0.0) Q[idx] = -Q[idx];
+}
+
 unsigned grid_of(long total) {
   long b = (total + 255) / 256;
   if (b > 148L * 8) b = 148L * 8;
@@ -191,6 +275,13 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   if (o.switch_diis_err <= 0) o.switch_diis_err = 1e-5;
   if (o.diis_size <= 0) o.diis_size = 8;
   if (o.lindep <= 0) o.lindep = 1e-10;
+  if (o.conv_grad <= 0) o.conv_grad = 1e-7;      // RHF_GR_CON_DEFAULT (include/defaults.h:7)
+  if (o.conv_energy <= 0) o.conv_energy = 1e-10;  // RHF_EN_CON_DEFAULT (include/defaults.h:6)
+  if (o.converger != RIJK_CONV_DIIS && o.converger != RIJK_CONV_SOSCF)
+    return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: unknown converger %d", o.converger);
+  if (o.lbfgs_vectors < 0 || o.lbfgs_vectors > 32)
+    return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: lbfgs_vectors outside 0 .. 32");
+  const bool soscf = o.converger == RIJK_CONV_SOSCF;
   int rc = check_fock_args(ctx, nocc, o.precision);
   if (rc) return rc;
   if (o.diis_size > 32) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: diis_size above 32");
@@ -357,9 +448,9 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       cleanup();
       return rc;
     }
-    if (diag(pF) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the guess Fock matrix failed");
+    if (diag(pF, soscf) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the guess Fock matrix failed");
   } else {
-    if (diag(pH) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
+    if (diag(pH, soscf) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
   }
   density(pD);
 
@@ -382,105 +473,275 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   double t_build = 0.0, t_diis = 0.0, t_diag = 0.0;
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto msec = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
-  for (int it = 0; it < o.max_iter; ++it) {
-    auto ta = now();
-    if ((rc = build(prec))) {
+  if (soscf) {
+    // the reference's RHF iteration (src/SCF.cpp:125-174) with its SOSCF engine
+    const long nv = nm - nocc, dim = nocc * nv, dimc = std::max<long>(dim, 1);
+    const int mvec = o.lbfgs_vectors > 0 ? o.lbfgs_vectors
+                                         : static_cast<int>(std::min<long>(nm, std::min(20, o.max_iter)));
+    const size_t nmm = static_cast<size_t>(nm) * nm;
+    DeviceBuf lb, qrw;
+    int lw_qr = 0, lw_or = 0;
+    if ((rc = ensure(ctx, lb, ((2 * static_cast<size_t>(mvec) + 8) * dimc + 2 * nmm + 2 * nm) * sizeof(double),
+                     "scf L-BFGS"))) {
       cleanup();
       return rc;
     }
-    // energy and DIIS error X^T (F D S - S D F) X
-    reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
-    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pF, ni, pD, ni, &zero, pT1, ni);   // F D
-    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pT1, ni, pS, ni, &zero, pT2, ni);  // F D S
-    k_antisym<<<grid_of(nn), 256, 0, s>>>(pT2, n, pT1);                                            // FDS - SDF
-    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, pT1, ni, pX, ni, &zero, pT2, ni);  // e X
-    double* slotE = rE + static_cast<size_t>(head) * nn;
-    double* slotF = rF + static_cast<size_t>(head) * nn;
-    cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT2, ni, &zero, slotE, nmi);  // X^T e X
-    cudaMemcpyAsync(slotF, pF, b_nn, cudaMemcpyDeviceToDevice, s);
-    reduce(AbsF{slotE}, nm * nm, 1, 1);
-    cudaEventRecord(ctx->ev3, s);
-    cudaMemcpyAsync(hout.data(), pOut, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf iteration")) || (rc = check_device_error(ctx))) {
+    double* g = static_cast<double*>(lb.p);  // gradient 4 F_ai, [i][a]
+    double* hd = g + dimc;                    // diagonal Hessian 4 (F_aa - F_ii)
+    double* q = hd + dimc;                    // two-loop work vector
+    double* sv = q + dimc;                    // the step before scaling
+    double* xs = sv + dimc;                   // the step applied
+    double* gprev = xs + dimc;
+    double* ysc = gprev + dimc;               // g - gprev
+    double* Yv = ysc + dimc;                  // mvec gradient differences
+    double* Sv = Yv + mvec * dimc;            // mvec steps, slot mvec = the last step taken
+    double* Fmo = Sv + (mvec + 1) * dimc;     // C^T F C
+    double* Rq = Fmo + nmm;                   // rotation, then its orthonormal rows
+    double* tau = Rq + nmm;
+    double* rdg = tau + nm;
+    cudaMemsetAsync(lb.p, 0, lb.bytes, s);
+    if (cusolverDnDgeqrf_bufferSize(cs, nmi, nmi, Rq, nmi, &lw_qr) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnDorgqr_bufferSize(cs, nmi, nmi, nmi, Rq, nmi, tau, &lw_or) != CUSOLVER_STATUS_SUCCESS) {
+      release(lb);
+      return fail(RIJK_ERR_SOLVER, "QR buffer query failed");
+    }
+    const int lwq = std::max(std::max(lw_qr, lw_or), 1);
+    if ((rc = ensure(ctx, qrw, static_cast<size_t>(lwq) * sizeof(double), "scf QR work"))) {
+      release(lb);
       cleanup();
       return rc;
     }
-    ms_fock += elapsed(ctx->ev0, ctx->ev2);
-    auto tb = now();
-    t_build += msec(ta, tb);
-    E = hout[0] + e_nuc;
-    err = hout[1];
-    if (result->history_len < 128) {
-      result->history_energy[result->history_len] = E;
-      result->history_diis_err[result->history_len] = err;
-      result->history_mixed[result->history_len] = prec == RIJK_PREC_MIXED ? 1 : 0;
-      ++result->history_len;
-    }
-    bool stalled = false;
-    if (prec == RIJK_PREC_MIXED) {
-      if (err < best_err * 0.9) {
-        best_err = err;
-        since_best = 0;
-      } else {
-        ++since_best;
-      }
-      // the split-BF16 rounding noise can put a floor under the DIIS error: stop waiting for it
-      stalled = since_best >= 5 || nmix >= o.max_iter / 2;
-    }
-    if (prec == RIJK_PREC_MIXED && (err < o.switch_diis_err || stalled)) {
-      // switch to the FP64 form: rebuild F for this same density and restart DIIS (unless the
-      // caller keeps the mixed-phase vectors)
-      prec = RIJK_PREC_FP64;
-      if (!o.diis_keep_on_switch) {
-        m = 0;
-        head = 0;
-      }
-      --it;
-      continue;
-    }
-    m = m < m_max ? m + 1 : m_max;
-    head = (head + 1) % m_max;
-    // Pulay B matrix over the stored error vectors
-    std::vector<double> Bm(static_cast<size_t>(m) * m);
-    {
-      int slots[32];
-      for (int i = 0; i < m; ++i) slots[i] = (head - m + i + m_max) % m_max;
-      for (int i = 0; i < m; ++i)
-        for (int j = 0; j <= i; ++j)
-          reduce(DotF{rE + static_cast<size_t>(slots[i]) * nn, rE + static_cast<size_t>(slots[j]) * nn}, nm * nm, 0,
-                 2 + i * (i + 1) / 2 + j);
-      std::vector<double> tmp(kOutSlots);
-      cudaMemcpyAsync(tmp.data(), pOut, kOutSlots * sizeof(double), cudaMemcpyDeviceToHost, s);
-      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf DIIS"))) {
+    double* pQw = static_cast<double*>(qrw.p);
+    auto fail2 = [&](int code, const char* msg) {
+      release(lb);
+      release(qrw);
+      return fail(code, msg);
+    };
+    const unsigned gd = grid_of(dim);
+    const bool guess_diag = o.guess_dm && o.guess_rows && o.guess_nrows > 0;
+    const double eps = std::numeric_limits<double>::epsilon();
+    std::vector<double> rho(mvec, 0.0);
+    double E_old = 1e15;
+    int step_num = 0, pair_num = 0;
+    bool have_rms = false;
+    for (int it = 0; it < o.max_iter; ++it) {
+      auto ta = now();
+      if ((rc = build(prec))) {
+        release(lb);
+        release(qrw);
         cleanup();
         return rc;
       }
-      for (int i = 0; i < m; ++i)
-        for (int j = 0; j <= i; ++j) Bm[i * m + j] = Bm[j * m + i] = tmp[2 + i * (i + 1) / 2 + j];
-      std::vector<double> c;
-      if (!diis_coefficients(Bm, m, c)) {
-        c.assign(m, 0.0);
-        c[m - 1] = 1.0;
+      reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, pF, ni, pC, ni, &zero, pT1, ni);     // F C
+      cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pC, ni, pT1, ni, &zero, Fmo, nmi);  // C^T F C
+      k_soscf_grad<<<gd, 256, 0, s>>>(Fmo, nm, nocc, g, hd);
+      reduce(AbsF{g}, dim, 1, 1);
+      if (step_num > 0) {  // curvature pair candidate (src/l-bfgs_2_1.cpp:44-61)
+        k_sub<<<gd, 256, 0, s>>>(g, gprev, dim, ysc);
+        reduce(DotF{Sv + mvec * dimc, ysc}, dim, 0, 2);
+        reduce(DotF{ysc, ysc}, dim, 0, 3);
       }
-      for (int i = 0; i < m; ++i)
-        k_axpy_set<<<grid_of(nn), 256, 0, s>>>(c[i], rF + static_cast<size_t>(slots[i]) * nn, nn, pFex, i == 0);
+      cudaMemcpyAsync(hout.data(), pOut, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
+      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf iteration")) || (rc = check_device_error(ctx))) {
+        release(lb);
+        release(qrw);
+        cleanup();
+        return rc;
+      }
+      ms_fock += elapsed(ctx->ev0, ctx->ev2);
+      auto tb = now();
+      t_build += msec(ta, tb);
+      E = hout[0] + e_nuc;
+      err = hout[1];
+      if (have_rms) rms = std::sqrt(hout[5] / static_cast<double>(nn));
+      if (result->history_len < 128) {
+        result->history_energy[result->history_len] = E;
+        result->history_diis_err[result->history_len] = err;
+        result->history_mixed[result->history_len] = prec == RIJK_PREC_MIXED ? 1 : 0;
+        ++result->history_len;
+      }
+      if (prec == RIJK_PREC_MIXED) {
+        if (err < best_err * 0.9) {
+          best_err = err;
+          since_best = 0;
+        } else {
+          ++since_best;
+        }
+        if (err < o.switch_diis_err || since_best >= 5 || nmix >= o.max_iter / 2) {
+          // to the FP64 form: rebuild F for the same orbitals, restart the L-BFGS history
+          prec = RIJK_PREC_FP64;
+          step_num = 0;
+          E_old = 1e15;
+          --it;
+          continue;
+        }
+      } else if (err < o.conv_grad || std::fabs(E - E_old) < o.conv_energy) {  // src/SCF.cpp:145-156
+        converged = true;
+        break;
+      }
+      auto tc = now();
+      if (it == 0 && !guess_diag) {  // first iteration: plain diagonalisation (src/SCF.cpp:160-166)
+        if (diag(pF, true) != RIJK_OK) return fail2(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
+        density(pDn);
+        reduce(DiffSqF{pDn, pD}, nn, 0, 5);
+        std::swap(pD, pDn);
+        have_rms = true;
+        E_old = E;
+        t_diag += msec(tc, now());
+        continue;
+      }
+      // L-BFGS two-loop step with the diagonal Hessian (src/l-bfgs_2_1.cpp:30-126)
+      if (step_num == 0) pair_num = 0;
+      if (step_num > 0) {
+        const double sy = hout[2], yy = hout[3];
+        if (sy > eps * yy) {
+          const int slot = pair_num % mvec;
+          cudaMemcpyAsync(Yv + slot * dimc, ysc, dim * sizeof(double), cudaMemcpyDeviceToDevice, s);
+          cudaMemcpyAsync(Sv + slot * dimc, Sv + mvec * dimc, dim * sizeof(double), cudaMemcpyDeviceToDevice, s);
+          rho[slot] = 1.0 / sy;
+          ++pair_num;
+        }
+      }
+      const int vec_num = std::min(pair_num, mvec);
+      cudaMemcpyAsync(q, g, dim * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(gprev, g, dim * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      for (int i = 0; i < vec_num; ++i) {  // alpha_i = rho s_k . q ; q -= alpha_i y_k (newest first)
+        const int k = (pair_num - i - 1) % mvec;
+        reduce(DotF{Sv + k * dimc, q}, dim, 0, 10 + i);
+        k_axpy_dev<<<gd, 256, 0, s>>>(q, Yv + k * dimc, dim, pOut, 10 + i, -rho[k], -1, 0.0);
+      }
+      k_div<<<gd, 256, 0, s>>>(q, hd, dim, sv);
+      for (int i = 0; i < vec_num; ++i) {  // beta = rho y_k . s ; s += (alpha - beta) s_k (oldest first)
+        const int k = (pair_num - vec_num + i) % mvec;
+        reduce(DotF{Yv + k * dimc, sv}, dim, 0, 50 + i);
+        k_axpy_dev<<<gd, 256, 0, s>>>(sv, Sv + k * dimc, dim, pOut, 10 + (vec_num - i - 1), rho[k], 50 + i, -rho[k]);
+      }
+      reduce(AbsF{sv}, dim, 1, 4);
+      k_zoom<<<gd, 256, 0, s>>>(sv, dim, pOut, 4, 6, 0.1, xs, Sv + mvec * dimc);  // x_max_soscf = 0.1
+      ++step_num;
+      auto td = now();
+      t_diis += msec(tc, td);
+      // orbitals <- (orthonormalised I + X - X^T) orbitals (src/converger_2_1.cpp:105-123)
+      k_rot_build<<<grid_of(nm * nm), 256, 0, s>>>(xs, nm, nocc, Rq);
+      if (cusolverDnDgeqrf(cs, nmi, nmi, Rq, nmi, tau, pQw, lwq, pInfo) != CUSOLVER_STATUS_SUCCESS)
+        return fail2(RIJK_ERR_SOLVER, "geqrf of the rotation failed");
+      k_copy_diag<<<grid_of(nm), 256, 0, s>>>(Rq, nm, rdg);
+      if (cusolverDnDorgqr(cs, nmi, nmi, nmi, Rq, nmi, tau, pQw, lwq, pInfo) != CUSOLVER_STATUS_SUCCESS)
+        return fail2(RIJK_ERR_SOLVER, "orgqr of the rotation failed");
+      k_sign_cols<<<grid_of(nm * nm), 256, 0, s>>>(Rq, nm, rdg);
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, nmi, &one, pC, ni, Rq, nmi, &zero, pT1, ni);  // C Q
+      cudaMemcpyAsync(pC, pT1, static_cast<size_t>(n) * nm * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      density(pDn);
+      reduce(DiffSqF{pDn, pD}, nn, 0, 5);
+      std::swap(pD, pDn);
+      have_rms = true;
+      E_old = E;
+      t_diag += msec(td, now());
     }
-    auto tc = now();
-    t_diis += msec(tb, tc);
-    if (diag(pFex) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
-    density(pDn);
-    reduce(DiffSqF{pDn, pD}, nn, 0, 0);
-    cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
-    if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf density"))) {
-      cleanup();
-      return rc;
-    }
-    rms = std::sqrt(hout[0] / static_cast<double>(nn));
-    t_diag += msec(tc, now());
-    std::swap(pD, pDn);
-    if (rms < o.conv_dm_rms && prec == RIJK_PREC_FP64) {
-      converged = true;
-      break;
+    release(lb);
+    release(qrw);
+  } else {
+    for (int it = 0; it < o.max_iter; ++it) {
+      auto ta = now();
+      if ((rc = build(prec))) {
+        cleanup();
+        return rc;
+      }
+      // energy and DIIS error X^T (F D S - S D F) X
+      reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pF, ni, pD, ni, &zero, pT1, ni);   // F D
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pT1, ni, pS, ni, &zero, pT2, ni);  // F D S
+      k_antisym<<<grid_of(nn), 256, 0, s>>>(pT2, n, pT1);                                            // FDS - SDF
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, pT1, ni, pX, ni, &zero, pT2, ni);  // e X
+      double* slotE = rE + static_cast<size_t>(head) * nn;
+      double* slotF = rF + static_cast<size_t>(head) * nn;
+      cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT2, ni, &zero, slotE, nmi);  // X^T e X
+      cudaMemcpyAsync(slotF, pF, b_nn, cudaMemcpyDeviceToDevice, s);
+      reduce(AbsF{slotE}, nm * nm, 1, 1);
+      cudaEventRecord(ctx->ev3, s);
+      cudaMemcpyAsync(hout.data(), pOut, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf iteration")) || (rc = check_device_error(ctx))) {
+        cleanup();
+        return rc;
+      }
+      ms_fock += elapsed(ctx->ev0, ctx->ev2);
+      auto tb = now();
+      t_build += msec(ta, tb);
+      E = hout[0] + e_nuc;
+      err = hout[1];
+      if (result->history_len < 128) {
+        result->history_energy[result->history_len] = E;
+        result->history_diis_err[result->history_len] = err;
+        result->history_mixed[result->history_len] = prec == RIJK_PREC_MIXED ? 1 : 0;
+        ++result->history_len;
+      }
+      bool stalled = false;
+      if (prec == RIJK_PREC_MIXED) {
+        if (err < best_err * 0.9) {
+          best_err = err;
+          since_best = 0;
+        } else {
+          ++since_best;
+        }
+        // the split-BF16 rounding noise can put a floor under the DIIS error: stop waiting for it
+        stalled = since_best >= 5 || nmix >= o.max_iter / 2;
+      }
+      if (prec == RIJK_PREC_MIXED && (err < o.switch_diis_err || stalled)) {
+        // switch to the FP64 form: rebuild F for this same density and restart DIIS (unless the
+        // caller keeps the mixed-phase vectors)
+        prec = RIJK_PREC_FP64;
+        if (!o.diis_keep_on_switch) {
+          m = 0;
+          head = 0;
+        }
+        --it;
+        continue;
+      }
+      m = m < m_max ? m + 1 : m_max;
+      head = (head + 1) % m_max;
+      // Pulay B matrix over the stored error vectors
+      std::vector<double> Bm(static_cast<size_t>(m) * m);
+      {
+        int slots[32];
+        for (int i = 0; i < m; ++i) slots[i] = (head - m + i + m_max) % m_max;
+        for (int i = 0; i < m; ++i)
+          for (int j = 0; j <= i; ++j)
+            reduce(DotF{rE + static_cast<size_t>(slots[i]) * nn, rE + static_cast<size_t>(slots[j]) * nn}, nm * nm, 0,
+                   2 + i * (i + 1) / 2 + j);
+        std::vector<double> tmp(kOutSlots);
+        cudaMemcpyAsync(tmp.data(), pOut, kOutSlots * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf DIIS"))) {
+          cleanup();
+          return rc;
+        }
+        for (int i = 0; i < m; ++i)
+          for (int j = 0; j <= i; ++j) Bm[i * m + j] = Bm[j * m + i] = tmp[2 + i * (i + 1) / 2 + j];
+        std::vector<double> c;
+        if (!diis_coefficients(Bm, m, c)) {
+          c.assign(m, 0.0);
+          c[m - 1] = 1.0;
+        }
+        for (int i = 0; i < m; ++i)
+          k_axpy_set<<<grid_of(nn), 256, 0, s>>>(c[i], rF + static_cast<size_t>(slots[i]) * nn, nn, pFex, i == 0);
+      }
+      auto tc = now();
+      t_diis += msec(tb, tc);
+      if (diag(pFex) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
+      density(pDn);
+      reduce(DiffSqF{pDn, pD}, nn, 0, 0);
+      cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
+      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf density"))) {
+        cleanup();
+        return rc;
+      }
+      rms = std::sqrt(hout[0] / static_cast<double>(nn));
+      t_diag += msec(tc, now());
+      std::swap(pD, pDn);
+      if (rms < o.conv_dm_rms && prec == RIJK_PREC_FP64) {
+        converged = true;
+        break;
+      }
     }
   }
   // final FP64 build at the converged density: the energy reported is consistent with D

@@ -25,6 +25,7 @@ ERR_ARG, ERR_STATE, ERR_CUDA, ERR_ALLOC, ERR_SOLVER, ERR_TIMEOUT, ERR_NUMERIC, E
 METRIC_INVSQRT, METRIC_CHOLESKY = 0, 1
 LAYOUT_NOPT_FULL, LAYOUT_PACKED = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+CONV_DIIS, CONV_SOSCF = 0, 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -60,7 +61,9 @@ class ScfOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv_dm_rms", ctypes.c_double), ("precision", ctypes.c_int),
                 ("switch_diis_err", ctypes.c_double), ("diis_size", ctypes.c_int),
                 ("diis_keep_on_switch", ctypes.c_int), ("lindep", ctypes.c_double),
-                ("guess_dm", _dp), ("guess_rows", _dp), ("guess_nrows", ctypes.c_long)]
+                ("guess_dm", _dp), ("guess_rows", _dp), ("guess_nrows", ctypes.c_long),
+                ("converger", ctypes.c_int), ("conv_grad", ctypes.c_double), ("conv_energy", ctypes.c_double),
+                ("lbfgs_vectors", ctypes.c_int)]
 
 
 class ScfResult(ctypes.Structure):
@@ -262,12 +265,16 @@ class FockBuilder:
         self._check(lib().rijk_fock_device(self._h, _vp(dD), _vp(dMO), int(n_c), _vp(dJ), _vp(dK), precision))
 
     def scf(self, H, S, n_c, e_nuc, precision=PREC_FP64, conv_dm_rms=1e-10, switch_diis_err=1e-5, max_iter=100,
-            diis_size=8, guess=None, diis_keep_on_switch=False):
+            diis_size=8, guess=None, diis_keep_on_switch=False, converger=CONV_DIIS, conv_grad=1e-7,
+            conv_energy=1e-10, lbfgs_vectors=0):
         """RHF on the GPU (rijk_scf); guess = (D0, R) with D0 = R^T R (e.g. SystemIntegrals.sad()),
-        None for the core-Hamiltonian start.  Returns (E, MO rows, result dict)."""
+        None for the core-Hamiltonian start; converger CONV_DIIS or CONV_SOSCF (the reference's
+        L-BFGS orbital rotations, converged on max|4 F_ai| < conv_grad or |dE| < conv_energy).
+        Returns (E, MO rows, result dict)."""
         n = self.n
         o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1 if diis_keep_on_switch else 0,
                     1e-10)
+        o.converger, o.conv_grad, o.conv_energy, o.lbfgs_vectors = converger, conv_grad, conv_energy, lbfgs_vectors
         if guess is not None:
             gD, gR = _c(guess[0]), _c(guess[1])
             o.guess_dm, o.guess_rows, o.guess_nrows = _p(gD), _p(gR), gR.shape[0]

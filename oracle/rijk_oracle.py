@@ -305,3 +305,107 @@ def scf_rhf(S, H, RI_AA, Vm05, n_occ, Enuc, conv_dm=1e-10, max_iter=100, diis_n=
             E = rhf_energy(F, H, DM, Enuc)
             return E, MO, DM, F, it
     return E, MO, DM, F, max_iter
+
+
+# ----------------------------------------------------- SOSCF converger ------
+def lbfgs_step(st, g, h, x_max=0.1):
+    """l_bfgs_engine::step as the reference builds it (LBFGS_RETURN_STEP, LBFGS_CALC_HESS with a
+    no-op Hessian callback; src/l-bfgs_2_1.cpp:30-126, Makefile DEFINITIONS): two-loop recursion
+    over the accepted curvature pairs with the diagonal Hessian h (not inverted), step scaled so
+    that no angle exceeds x_max.  `st` holds the engine state between calls."""
+    m = st["m"]
+    if st["step"] == 0:
+        st["pairs"] = 0
+    if m > 0 and st["step"] > 0:                                        # :44-61
+        y = g - st["gprev"]
+        sy, yy = float(st["last"] @ y), float(y @ y)
+        if sy > np.finfo(float).eps * yy:
+            k = st["pairs"] % m
+            st["Y"][k], st["S"][k], st["rho"][k] = y, st["last"].copy(), 1.0 / sy
+            st["pairs"] += 1
+    P = st["pairs"]
+    vec = min(P, m)
+    q = g.copy()
+    st["gprev"] = g.copy()
+    alpha = np.zeros(vec)
+    for i in range(vec):                                                # :75-82
+        k = (P - i - 1) % m
+        alpha[i] = st["rho"][k] * float(st["S"][k] @ q)
+        q -= alpha[i] * st["Y"][k]
+    s = q / h                                                           # :85
+    for i in range(vec):                                                # :87-95
+        k = (P - vec + i) % m
+        beta = st["rho"][k] * float(st["Y"][k] @ s)
+        s += (alpha[vec - i - 1] - beta) * st["S"][k]
+    smax = float(np.max(np.abs(s))) if s.size else 0.0
+    zoom = -x_max / smax if smax > x_max else -1.0                      # :96-102
+    x = s * zoom                                                        # :105-107
+    st["last"] = x.copy()                                               # :118-121
+    st["step"] += 1
+    return x
+
+
+def gram_schmidt_rows(R):
+    """ortogonalization (src/matr.cpp:1001-1016): rows made orthonormal in order."""
+    R = R.copy()
+    for i in range(R.shape[0]):
+        R[i] /= np.sqrt(R[i] @ R[i])
+        R[i + 1:] -= np.outer(R[i + 1:] @ R[i], R[i])
+    return R
+
+
+def scf_soscf(S, H, RI_AA, Vm05, n_occ, Enuc, e_conv=1e-10, g_conv=1e-7, max_iter=100, jk=None, guess=None,
+              lindep=1e-10):
+    """The reference's RHF loop (src/SCF.cpp:125-174) with its SOSCF engine
+    (src/converger_2_1.cpp:55-125): g_ia = 4 F_ai and H_ia = 4 (e_a - e_i) in the MO basis,
+    L-BFGS step, orbitals rotated by the Gram-Schmidt-orthonormalised I + X - X^T; the first
+    iteration diagonalises instead unless a guess was given; converged on max|g| < g_conv or
+    |dE| < e_conv.  Canonical orthogonalisation X and the starts are those of scf_rhf.
+    Returns (E, MO, history [(E, max|g|) per Fock build], converged)."""
+    n = S.shape[0]
+    s, U = np.linalg.eigh(S)
+    keep = s >= lindep
+    X = U[:, keep] / np.sqrt(s[keep])
+    if jk is None:
+        jk = lambda D, MO, nr=n_occ: dm_to_f_transform_ri(RI_AA, Vm05, D, MO, nr, n)
+
+    def diag(F):
+        e, Cp = np.linalg.eigh(X.T @ F @ X)
+        return (X @ Cp).T
+
+    if guess is not None:
+        J0, K0 = jk(guess[0], guess[1], guess[1].shape[0])
+        MO = diag(calc_f_ao(H, J0, K0))
+    else:
+        MO = diag(H)
+    nm = MO.shape[0]
+    nv = nm - n_occ
+    m = min(nm, 20, max_iter)
+    st = {"m": m, "step": 0, "pairs": 0, "gprev": np.zeros(n_occ * nv), "last": np.zeros(n_occ * nv),
+          "Y": np.zeros((m, n_occ * nv)), "S": np.zeros((m, n_occ * nv)), "rho": np.zeros(m)}
+    E_old, hist, converged = 1e15, [], False
+    for it in range(max_iter):
+        DM = gen_hf_dm(MO, n, n_occ)
+        J, K = jk(DM, MO)
+        F = calc_f_ao(H, J, K)
+        E = rhf_energy(F, H, DM, Enuc)
+        Fmo = MO @ F @ MO.T
+        g = 4.0 * Fmo[n_occ:, :n_occ].T.reshape(-1)                      # orb_grad_calc
+        e = np.diag(Fmo)
+        h = 4.0 * (e[None, n_occ:] - e[:n_occ, None]).reshape(-1)       # orb_hess_calc
+        gmax = float(np.max(np.abs(g))) if g.size else 0.0
+        hist.append((E, gmax))
+        if gmax < g_conv or abs(E - E_old) < e_conv:
+            converged = True
+            break
+        if it == 0 and guess is None:
+            MO = diag(F)
+            E_old = E
+            continue
+        x = lbfgs_step(st, g, h)
+        R = np.eye(nm)
+        R[:n_occ, n_occ:] = x.reshape(n_occ, nv)
+        R[n_occ:, :n_occ] = -x.reshape(n_occ, nv).T
+        MO = gram_schmidt_rows(R) @ MO
+        E_old = E
+    return E, MO, hist, converged

@@ -118,3 +118,29 @@ def test_sad_guess_density_and_factor_rows():
     Vm05, _ = O.s05_calc(si.V)
     E, MO, DM, F, it = O.scf_rhf(si.S, si.H, si.I3, Vm05, si.nocc, si.Enuc, guess=(D0, R))
     assert abs(E - p["energy"]) < 2e-9
+
+
+def test_soscf_converger_restatement_reaches_reference_energy():
+    """The restatement of the reference's own converger (SOSCF with L-BFGS, src/SCF.cpp:125-174)
+    lands on the logged C2H4 energy from the core guess and from the SAD start."""
+    p = [q for q in GOLD["pins"] if q["name"] == "c2h4"][0]
+    si = ints.SystemIntegrals(_mol(p), p["basis"], p["aux"], layout=ints.LAYOUT_NOPT_FULL)
+    Vm05, _ = O.s05_calc(si.V)
+    E, MO, hist, conv = O.scf_soscf(si.S, si.H, si.I3, Vm05, si.nocc, si.Enuc)
+    assert conv and abs(E - p["energy"]) < 2e-9, (E, p["energy"])
+    Eg, _, hg, convg = O.scf_soscf(si.S, si.H, si.I3, Vm05, si.nocc, si.Enuc, guess=si.sad())
+    assert convg and abs(Eg - p["energy"]) < 2e-9 and len(hg) < len(hist)
+
+
+def test_gram_schmidt_rows_is_qr_with_positive_diagonal():
+    """Row-wise Gram-Schmidt of I + X - X^T equals Q^T of the QR factorisation of its transpose
+    with R's diagonal made positive (the form the device code uses)."""
+    rng = np.random.default_rng(3)
+    no, nv = 5, 9
+    x = 0.1 * rng.normal(size=(no, nv))
+    R = np.eye(no + nv)
+    R[:no, no:] = x
+    R[no:, :no] = -x.T
+    Q, Rr = np.linalg.qr(R.T)
+    Q = Q * np.sign(np.diag(Rr))
+    np.testing.assert_allclose(O.gram_schmidt_rows(R), Q.T, atol=1e-13)
