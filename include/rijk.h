@@ -77,6 +77,7 @@ typedef struct {
   char stage_names[12][24];
   double ms_setup_ints;   /* last rijk_set_basis: device time of the integral kernels          */
   int kernels_setup_ints; /* integral kernels it launched                                    */
+  long q0, nq;            /* aux functions [q0, q0 + nq) held (all of them unless sliced)      */
 } rijk_stats_t;
 
 int rijk_create(rijk_ctx** ctx, int device);
@@ -129,6 +130,14 @@ int rijk_eri3c(rijk_ctx* ctx, const rijk_basis_t* orb, const rijk_basis_t* aux, 
  * Equivalent to rijk_set_metric + rijk_set_aux_range + rijk_set_3c on the same integrals. */
 int rijk_set_basis(rijk_ctx* ctx, const rijk_basis_t* orb, const rijk_basis_t* aux, int metric_form, long q0,
                    long q1);
+
+/* The fitted tensor on disk (no reference counterpart: NOPT rebuilds RI_AA in every run).
+ * rijk_save writes the metric factor and B (or the aux slice held) of a set-up context to a file;
+ * rijk_load reads one into any context, which can then run Fock builds, rijk_grad and the MO
+ * tensor calls without integrals.  The file carries a checksum: a damaged or truncated file gives
+ * RIJK_ERR_ARG and leaves the context unchanged. */
+int rijk_save(rijk_ctx* ctx, const char* path);
+int rijk_load(rijk_ctx* ctx, const char* path);
 
 /* Drop-in for DM_to_F_transform_RI(J, K, DM, MO, n_c, n_ao): host pointers, synchronous. */
 int rijk_fock(rijk_ctx* ctx, const double* DM, const double* MO, long n_c, double* J, double* K, int precision);

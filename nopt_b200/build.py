@@ -30,6 +30,7 @@ CUDA_SOURCES = [
     "rijk/rijk_noalloc.cu",
     "rijk/k_eri.cu",
     "rijk/k_mo_ri.cu",
+    "rijk/rijk_cache.cu",
 ]
 
 

@@ -303,6 +303,8 @@ RIJK_API int rijk_set_profiling(rijk_ctx* ctx, int on) {
 RIJK_API int rijk_get_stats(const rijk_ctx* ctx, rijk_stats_t* out) {
   if (!ctx || !out) return RIJK_ERR_ARG;
   *out = ctx->stats;
+  out->q0 = ctx->q0;
+  out->nq = ctx->nq;
   return RIJK_OK;
 }
 

@@ -40,7 +40,7 @@ class Stats(ctypes.Structure):
                 ("bytes_b_mixed", ctypes.c_long), ("kernels_last_fock", ctypes.c_int),
                 ("profiled_stages", ctypes.c_int), ("ms_stage", ctypes.c_double * 12),
                 ("stage_names", (ctypes.c_char * 24) * 12), ("ms_setup_ints", ctypes.c_double),
-                ("kernels_setup_ints", ctypes.c_int)]
+                ("kernels_setup_ints", ctypes.c_int), ("q0", ctypes.c_long), ("nq", ctypes.c_long)]
 
 
 class BasisT(ctypes.Structure):
@@ -110,6 +110,8 @@ def lib():
         L.rijk_mo_calc.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long, _dp, _dp, _dp, _dp, _dp]
         L.rijk_mo_ints_aaag.argtypes = [_vp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
         L.rijk_soscf_hess_ints.argtypes = [_vp, _dp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
+        L.rijk_save.argtypes = [_vp, ctypes.c_char_p]
+        L.rijk_load.argtypes = [_vp, ctypes.c_char_p]
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
@@ -138,7 +140,6 @@ class FockBuilder:
         if rc != OK:
             raise RijkError(rc, "rijk_create(device=%d) failed" % device)
         self._h = h
-        self._q = None  # aux slice (q0, q1) held, None for all
         self.n = self.naux = None
 
     def close(self):
@@ -176,12 +177,10 @@ class FockBuilder:
         V = _c(V)
         self._check(lib().rijk_set_metric(self._h, _p(V), V.shape[0], form))
         self.naux = V.shape[0]
-        self._q = None
 
     def set_aux_range(self, q0, q1):
         """Hold only aux functions [q0, q1): Fock builds then return that slice's partial J, K."""
         self._check(lib().rijk_set_aux_range(self._h, int(q0), int(q1)))
-        self._q = (int(q0), int(q1))
 
     def set_3c(self, I3, n, layout=LAYOUT_PACKED):
         I3 = _c(I3)
@@ -192,8 +191,7 @@ class FockBuilder:
         """gen_RI_AA on the GPU: integrals, metric factor and fitted tensor from two Basis objects."""
         bo, ba = basis_t(orb), basis_t(aux)
         self._check(lib().rijk_set_basis(self._h, ctypes.byref(bo), ctypes.byref(ba), metric_form, int(q0), int(q1)))
-        self._q = (int(q0), int(q1)) if q1 > 0 else None
-        self.n = orb.nbf
+        self.n, self.naux = orb.nbf, aux.nbf
 
     def eri2c(self, aux):
         """(P|Q) computed on the GPU (naux x naux)."""
@@ -210,6 +208,17 @@ class FockBuilder:
         out = np.empty(shape)
         self._check(lib().rijk_eri3c(self._h, ctypes.byref(bo), ctypes.byref(ba), layout, _p(out)))
         return out
+
+    def save(self, path):
+        """Write the metric factor and fitted tensor to a file (rijk_save)."""
+        self._check(lib().rijk_save(self._h, os.fsencode(path)))
+
+    def load(self, path):
+        """Read a file written by save into this context (rijk_load)."""
+        self._check(lib().rijk_load(self._h, os.fsencode(path)))
+        s = Stats()
+        self._check(lib().rijk_get_stats(self._h, ctypes.byref(s)))
+        self.n, self.naux = s.n, s.naux
 
     def mo_tensor(self, C1, C2):
         """(p a|Q) for the orbital rows of C1 and C2, shape (n1 * n2, naux)."""
@@ -248,7 +257,7 @@ class FockBuilder:
     def _naux(self):
         s = Stats()
         self._check(lib().rijk_get_stats(self._h, ctypes.byref(s)))
-        return s.naux if self._q is None else self._q[1] - self._q[0]
+        return s.nq
 
     def dm_to_f_transform_ri(self, DM, MO, n_c, precision=PREC_FP64, J=None, K=None):
         """(J, K) exactly as the reference's DM_to_F_transform_RI(J, K, DM, MO, n_c, n_ao)."""
