@@ -7,6 +7,8 @@
 //                                        summed while unpacking)
 // Both passes stream B once with 128-bit loads that bypass L1; reductions are warp
 // shuffles.  Algorithmic traffic: 2 * |B| bytes per build.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 
 #include "dmma.cuh"
@@ -94,8 +96,8 @@ __global__ void __launch_bounds__(J_THREADS) k_coulomb_j(const double* __restric
   reinterpret_cast<double2*>(Jpart + s * tile_elems)[e2] = make_double2(ax, ay);
 }
 
-int coulomb_nsplit(long tile_elems, long naux) {
-  long blocks = (tile_elems / 2 + J_THREADS - 1) / J_THREADS;
+int coulomb_nsplit(long tile_elems, long naux, int elems_per_thread) {
+  long blocks = (tile_elems / elems_per_thread + J_THREADS - 1) / J_THREADS;
   long want = (148L * 8 + blocks - 1) / blocks;  // about 8 CTAs per SM in flight
   if (want < 1) want = 1;
   if (want > 32) want = 32;
@@ -145,60 +147,82 @@ __device__ __forceinline__ uint4 ldg_stream_u4(const void* p) {
 // Element offset of packed element e (tile t = e / 4096) inside one aux function's Bmix block.
 __device__ __forceinline__ long mix_off(long e) { return (e >> 12) * 8192 + (e & 4095); }
 
-constexpr int WM_QB = 8;          // aux functions per CTA (each Dt load serves 8 of them)
-constexpr int WM_THREADS = 256;
+constexpr int WM_THREADS = 256;  // 8 warps; each warp reduces one aux function over the chunk at a time
+constexpr int WM_OCT = 1024;     // octets (8 elements) per chunk: two tiles, 32 KB of fp32 Dt in shared memory
+constexpr int WM_QR = 32;        // aux functions per CTA
 
+int coulomb_w_mixed_chunks(long ntile) { return static_cast<int>((ntile * TILE2 / 8 + WM_OCT - 1) / WM_OCT); }
+
+// wpart[c][q] = sum over octet chunk c (blockIdx.x) of Bmix[q][e] Dt[e], q in the WM_QR aux functions
+// of blockIdx.y.  The chunk's Dt is staged once as fp32 in two planes (elements 0-3 and 4-7 of each
+// octet), so a warp's 16-byte reads of it are conflict-free; each warp then streams one aux
+// function's hi/lo planes over the chunk with four octets per lane in flight and reduces by shuffle.
 __global__ void __launch_bounds__(WM_THREADS) k_coulomb_w_mixed(const __nv_bfloat16* __restrict__ Bmix,
                                                                  const double* __restrict__ Dt, long naux, long ntile,
-                                                                 long ntile2, double* __restrict__ w) {
-  const long q0 = static_cast<long>(blockIdx.x) * WM_QB;
+                                                                 long ntile2, double* __restrict__ wpart) {
+  __shared__ __align__(16) float sd[2][WM_OCT * 4];
   const long n8 = ntile * TILE2 / 8;
-  const long qstride = ntile2 * 2 * TILE2;
-  double acc[WM_QB];  // each group of 8 products is summed in fp32, the groups in fp64
-#pragma unroll
-  for (int j = 0; j < WM_QB; ++j) acc[j] = 0.0;
-  const __nv_bfloat16* qb[WM_QB];
-#pragma unroll
-  for (int j = 0; j < WM_QB; ++j) qb[j] = Bmix + (q0 + j < naux ? q0 + j : naux - 1) * qstride;
-  for (long e8 = threadIdx.x; e8 < n8; e8 += WM_THREADS) {
-    const long e = e8 * 8;
-    const long off = mix_off(e);
-    uint4 h[WM_QB], l[WM_QB];
-#pragma unroll
-    for (int j = 0; j < WM_QB; ++j) {
-      h[j] = ldg_stream_u4(qb[j] + off);
-      l[j] = ldg_stream_u4(qb[j] + off + TILE2);
-    }
-    const double4 d0 = *reinterpret_cast<const double4*>(Dt + e);
-    const double4 d1 = *reinterpret_cast<const double4*>(Dt + e + 4);
-    const float d[8] = {static_cast<float>(d0.x), static_cast<float>(d0.y), static_cast<float>(d0.z),
-                        static_cast<float>(d0.w), static_cast<float>(d1.x), static_cast<float>(d1.y),
-                        static_cast<float>(d1.z), static_cast<float>(d1.w)};
-#pragma unroll
-    for (int j = 0; j < WM_QB; ++j) {
-      float b[8];
-      bf16x8_sum(h[j], l[j], b);
-      float t = 0.f;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) t = fmaf(b[k], d[k], t);
-      acc[j] += static_cast<double>(t);
-    }
-  }
-  __shared__ double red[WM_QB][WM_THREADS / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int j = 0; j < WM_QB; ++j) {
-    double v = warp_sum(acc[j]);
-    if (lane == 0) red[j][warp] = v;
+  const long c0 = static_cast<long>(blockIdx.x) * WM_OCT;
+  const int cnt = static_cast<int>(n8 - c0 < WM_OCT ? n8 - c0 : WM_OCT);
+  const double4* D4 = reinterpret_cast<const double4*>(Dt + c0 * 8);
+  for (int i = threadIdx.x; i < 2 * cnt; i += WM_THREADS) {  // i = 2 * octet + half
+    const double4 d = D4[i];
+    reinterpret_cast<float4*>(sd[i & 1])[i >> 1] =
+        make_float4(static_cast<float>(d.x), static_cast<float>(d.y), static_cast<float>(d.z), static_cast<float>(d.w));
   }
   __syncthreads();
-  if (warp == 0) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long qstride = ntile2 * 2 * TILE2;
+  const long qa = static_cast<long>(blockIdx.y) * WM_QR;
+  const float4* s0 = reinterpret_cast<const float4*>(sd[0]);
+  const float4* s1 = reinterpret_cast<const float4*>(sd[1]);
+  for (int j = warp; j < WM_QR; j += WM_THREADS / 32) {
+    const long q = qa + j;
+    if (q >= naux) break;
+    const __nv_bfloat16* qb = Bmix + q * qstride;
+    double acc = 0.0;  // each octet's 8 products are summed in fp32, the octets in fp64
+    auto dot = [&](const uint4 h, const uint4 l, int o) {
+      float b[8];
+      bf16x8_sum(h, l, b);
+      const float4 d0 = s0[o], d1 = s1[o];
+      float t = b[0] * d0.x;
+      t = fmaf(b[1], d0.y, t);
+      t = fmaf(b[2], d0.z, t);
+      t = fmaf(b[3], d0.w, t);
+      t = fmaf(b[4], d1.x, t);
+      t = fmaf(b[5], d1.y, t);
+      t = fmaf(b[6], d1.z, t);
+      t = fmaf(b[7], d1.w, t);
+      acc += static_cast<double>(t);
+    };
+    int o = lane;
+    for (; o + 96 < cnt; o += 128) {
+      uint4 h[4], l[4];
 #pragma unroll
-    for (int j = 0; j < WM_QB; ++j) {
-      double v = lane < WM_THREADS / 32 ? red[j][lane] : 0.0;
-      v = warp_sum(v);
-      if (lane == 0 && q0 + j < naux) w[q0 + j] = v;
+      for (int u = 0; u < 4; ++u) {
+        const long off = mix_off((c0 + o + 32 * u) * 8);
+        h[u] = ldg_stream_u4(qb + off);
+        l[u] = ldg_stream_u4(qb + off + TILE2);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) dot(h[u], l[u], o + 32 * u);
     }
+    for (; o < cnt; o += 32) {
+      const long off = mix_off((c0 + o) * 8);
+      dot(ldg_stream_u4(qb + off), ldg_stream_u4(qb + off + TILE2), o);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) wpart[blockIdx.x * naux + q] = acc;
+  }
+}
+
+// w[q] = sum_c wpart[c][q], in chunk order (deterministic)
+__global__ void k_sum_chunks(const double* __restrict__ wpart, int nchunk, long naux, double* __restrict__ w) {
+  for (long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; q < naux;
+       q += static_cast<long>(gridDim.x) * blockDim.x) {
+    double v = 0.0;
+    for (int c = 0; c < nchunk; ++c) v += wpart[c * naux + q];
+    w[q] = v;
   }
 }
 
@@ -247,10 +271,13 @@ __global__ void __launch_bounds__(J_THREADS) k_coulomb_j_mixed(const __nv_bfloat
   *reinterpret_cast<double4*>(out + 4) = make_double4(acc[4], acc[5], acc[6], acc[7]);
 }
 
+// w needs room for (1 + coulomb_w_mixed_chunks(ntile)) * naux doubles: w, then the chunk partials.
 void launch_coulomb_w_mixed(const __nv_bfloat16* Bmix, const double* Dt, long naux, long ntile, long ntile2, double* w,
                             cudaStream_t s) {
-  unsigned grid = static_cast<unsigned>((naux + WM_QB - 1) / WM_QB);
-  k_coulomb_w_mixed<<<grid, WM_THREADS, 0, s>>>(Bmix, Dt, naux, ntile, ntile2, w);
+  const int chunks = coulomb_w_mixed_chunks(ntile);
+  dim3 grid(static_cast<unsigned>(chunks), static_cast<unsigned>((naux + WM_QR - 1) / WM_QR));
+  k_coulomb_w_mixed<<<grid, WM_THREADS, 0, s>>>(Bmix, Dt, naux, ntile, ntile2, w + naux);
+  k_sum_chunks<<<static_cast<unsigned>((naux + 255) / 256), 256, 0, s>>>(w + naux, chunks, naux, w);
 }
 
 void launch_coulomb_j_mixed(const __nv_bfloat16* Bmix, const double* w, long naux, long ntile, long ntile2,

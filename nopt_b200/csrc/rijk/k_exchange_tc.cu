@@ -545,10 +545,22 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   const long noccp = round_up(nocc, 16);
   const long kdim = naux * noccp;
   const long nb = nt2 / 2, ntile128 = nb * (nb + 1) / 2;
-  // split-K: chunk-aligned ranges, about 4 CTAs per SM in total, every split non-empty
+  // split-K: chunk-aligned ranges, at least ~4 CTAs per SM in total, every split non-empty; the
+  // split count is chosen in [want, 4 want] so that the CTAs fill whole waves (one CTA per SM)
   const long nchunks = (kdim + 63) / 64;
-  long want = std::max<long>(1, (4L * num_sms(ctx->device) + ntile128 - 1) / ntile128);
-  long per = std::max<long>(2, (nchunks + want - 1) / want);
+  const long sms = num_sms(ctx->device);
+  const long want = std::max<long>(1, (4L * sms + ntile128 - 1) / ntile128);
+  long best = want;
+  double best_eff = 0.0;
+  for (long sp = want; sp <= 4 * want && sp <= std::max<long>(1, nchunks / 2); ++sp) {
+    const long ctas = ntile128 * sp, waves = (ctas + sms - 1) / sms;
+    const double eff = static_cast<double>(ctas) / static_cast<double>(waves * sms);
+    if (eff > best_eff + 0.02) {  // prefer fewer splits unless the fill improves noticeably
+      best_eff = eff;
+      best = sp;
+    }
+  }
+  const long per = std::max<long>(2, (nchunks + best - 1) / best);
   const long kper = per * 64;
   const int nsplit = static_cast<int>((kdim + kper - 1) / kper);
   cudaStream_t s = ctx->stream;

@@ -138,9 +138,9 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
   cudaStream_t s = ctx->stream;
   int rc;
   int launches = 0;
-  const int nsJ = coulomb_nsplit(tile_elems, naux);
+  const int nsJ = coulomb_nsplit(tile_elems, naux, precision == RIJK_PREC_MIXED ? 8 : 2);
   if ((rc = ensure(ctx, ctx->Dt, tile_elems * sizeof(double), "Dt")) ||
-      (rc = ensure(ctx, ctx->w, naux * sizeof(double), "w")) ||
+      (rc = ensure(ctx, ctx->w, (1 + coulomb_w_mixed_chunks(ntile)) * naux * sizeof(double), "w")) ||  // w, partials
       (rc = ensure(ctx, ctx->Jpart, static_cast<size_t>(nsJ) * tile_elems * sizeof(double), "Jpart")))
     return rc;
   if (precision == RIJK_PREC_MIXED && (rc = mixed_prepare(ctx))) return rc;
@@ -168,7 +168,7 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
   }
   launch_unpack_sym(static_cast<double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, s);
   prof_mark(ctx, "unpack_j");
-  launches += 4;
+  launches += (precision == RIJK_PREC_MIXED ? 5 : 4) + (nsJ > 1 ? 1 : 0);  // pack, w (+ chunk sum), j, unpack (+ split sum)
   cudaEventRecord(ctx->ev1, s);
 
   if (nocc == 0) {

@@ -119,7 +119,10 @@ void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const
                                   long naux, long nt, long I0, long I1, double* B, cudaStream_t s);
 
 // ---- k_coulomb.cu
-int coulomb_nsplit(long tile_elems, long naux);
+// Q splits of the J pass: elems_per_thread = 2 (FP64 B, double2) or 8 (split-BF16 copy).
+int coulomb_nsplit(long tile_elems, long naux, int elems_per_thread);
+// Octet chunks of the mixed w pass; its w buffer holds (1 + chunks) * naux doubles.
+int coulomb_w_mixed_chunks(long ntile);
 void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s);
 void launch_coulomb_j(const double* B, const double* w, long naux, long tile_elems, int nsplit, double* Jpart,
                       cudaStream_t s);

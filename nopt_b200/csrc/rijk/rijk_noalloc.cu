@@ -80,7 +80,7 @@ RIJK_API int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ) 
                    "rijk_coulomb_noalloc: n_ao = %ld, naux = %ld need %ld bytes of scratch; the fixed scratch holds "
                    "%ld bytes (use rijk_fock_device for this size)",
                    n, naux, need_min * static_cast<long>(sizeof(double)), static_cast<long>(RIJK_NOALLOC_SCRATCH_BYTES));
-  int nsplit = coulomb_nsplit(tile_elems, naux);
+  int nsplit = coulomb_nsplit(tile_elems, naux, 2);
   const long fit = (kNoallocScratchDoubles - tile_elems - nauxr) / tile_elems;
   if (nsplit > fit) nsplit = static_cast<int>(fit);
 

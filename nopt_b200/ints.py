@@ -187,15 +187,17 @@ def set_threads(n):
 class SystemIntegrals:
     """All inputs of an RI-RHF calculation for one molecule."""
 
-    def __init__(self, mol, orb_basis, aux_basis, layout=LAYOUT_PACKED):
+    def __init__(self, mol, orb_basis, aux_basis, layout=LAYOUT_PACKED, ri_integrals=True):
+        """ri_integrals=False skips (P|Q) and (mu nu|P) on the host (V and I3 are then None), for
+        callers that form them on the GPU (FockBuilder.set_basis)."""
         self.mol = mol
         self.orb = Basis.for_molecule(orb_basis, mol)
         self.aux = Basis.for_molecule(aux_basis, mol)
         self.S = overlap(self.orb)
         self.H = kinetic(self.orb) + nuclear(self.orb, mol)
-        self.V = coulomb_2c(self.aux)
+        self.V = coulomb_2c(self.aux) if ri_integrals else None
         self.layout = layout
-        self.I3 = coulomb_3c(self.orb, self.aux, layout)
+        self.I3 = coulomb_3c(self.orb, self.aux, layout) if ri_integrals else None
         self.Enuc = mol.nuclear_repulsion()
         self.nocc = mol.nelec // 2
         self.orb_name, self.aux_name = orb_basis, aux_basis
