@@ -81,6 +81,7 @@ __global__ void k_split_c(const double* __restrict__ MO, long nocc, long n, long
 // ---------------------------------------------------------- K3: half-transform ----
 struct XformParams {
   int nt2, ntile2, naux, npairs, stages;
+  int c_resident;  // 1: all of C is loaded into shared memory once; stages then carry the A tiles only
   long kdim;  // naux * noccp
   __nv_bfloat16* XTh;
   __nv_bfloat16* XTl;
@@ -98,6 +99,13 @@ struct XformCfg {
   static constexpr uint32_t kAccCols = kTmemCols / 2;
   static int stages() { return std::min(6, static_cast<int>((kSmemBudget - 2048) / kStage)); }
   static size_t smem(int st) { return static_cast<size_t>(st) * kStage + 1024 + 256; }
+  // resident C: nt2 chunks of (hi, lo) planes kept for the whole kernel, A-only stages
+  __host__ __device__ static size_t c_bytes(int nt2) { return static_cast<size_t>(nt2) * 2 * kCBytes; }
+  static int stages_resident(int nt2) {
+    const long room = static_cast<long>(kSmemBudget) - 2048 - static_cast<long>(c_bytes(nt2));
+    return room > 0 ? std::min(6, static_cast<int>(room / kABytes)) : 0;
+  }
+  static size_t smem_resident(int st, int nt2) { return static_cast<size_t>(st) * kABytes + c_bytes(nt2) + 1024 + 256; }
 };
 
 template <int NOCCP>
@@ -107,12 +115,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
   const int S = p.stages;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * Cfg::kStage);
+  const bool cres = p.c_resident != 0;
+  const uint32_t stage_bytes = cres ? Cfg::kABytes : Cfg::kStage;
+  uint8_t* cbase = smem + S * stage_bytes;  // resident C (cres only)
+  uint64_t* full = reinterpret_cast<uint64_t*>(cbase + (cres ? Cfg::c_bytes(p.nt2) : 0));
   uint64_t* empty = full + S;
   uint64_t* tfull = empty + S;
   uint64_t* tempty = tfull + 2;
   uint64_t* drain = tempty + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  uint64_t* cfull = drain + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cfull + 1);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -126,6 +138,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&tempty[b], 4);
     }
     mbar_init(drain, 1);
+    mbar_init(cfull, 1);
     *abort = 0;
     fence_barrier_init();
   }
@@ -146,6 +159,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
+      if (cres) {  // every C chunk once: hi at + 0, lo at + kCBytes of chunk I
+        mbar_expect_tx(cfull, static_cast<uint32_t>(Cfg::c_bytes(p.nt2)));
+        for (int I = 0; I < p.nt2; ++I) {
+          uint8_t* c = cbase + static_cast<size_t>(I) * 2 * Cfg::kCBytes;
+          tma_load_2d(c, &mapC, cfull, I * 64, 0);
+          tma_load_2d(c + Cfg::kCBytes, &mapC, cfull, I * 64, NOCCP);
+        }
+      }
       for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
         const int Q = item / p.npairs, jp = item - Q * p.npairs;
         const int J0 = 2 * jp, J1 = J0 + 1;
@@ -155,8 +176,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             ok = false;
             break;
           }
-          uint8_t* st = smem + stage * Cfg::kStage;
-          mbar_expect_tx(&full[stage], Cfg::kStage);
+          uint8_t* st = smem + stage * stage_bytes;
+          mbar_expect_tx(&full[stage], stage_bytes);
           const int t0 = (I <= J0) ? tri2(J0, I) : tri2(I, J0);
           const int t1 = (I <= J0) ? tri2(J1, I) : tri2(I, J1);
           const int y0 = static_cast<int>((qbase + t0) * 128), y1 = static_cast<int>((qbase + t1) * 128);
@@ -164,8 +185,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tma_load_2d(st + 1 * kTileBytes, &mapB, &full[stage], 0, y1);        // A hi, group 1
           tma_load_2d(st + 2 * kTileBytes, &mapB, &full[stage], 0, y0 + 64);   // A lo, group 0
           tma_load_2d(st + 3 * kTileBytes, &mapB, &full[stage], 0, y1 + 64);   // A lo, group 1
-          tma_load_2d(st + Cfg::kABytes, &mapC, &full[stage], I * 64, 0);               // C hi
-          tma_load_2d(st + Cfg::kABytes + Cfg::kCBytes, &mapC, &full[stage], I * 64, NOCCP);  // C lo
+          if (!cres) {
+            tma_load_2d(st + Cfg::kABytes, &mapC, &full[stage], I * 64, 0);               // C hi
+            tma_load_2d(st + Cfg::kABytes + Cfg::kCBytes, &mapC, &full[stage], I * 64, NOCCP);  // C lo
+          }
           if (++stage == S) {
             stage = 0;
             phase ^= 1;
@@ -184,6 +207,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         uint32_t par = (s < stage) ? phase : (phase ^ 1);
         mbar_wait(&full[s], par, &never);
       }
+      if (cres) mbar_wait(cfull, 0, &never);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -196,6 +220,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       uint32_t tph[2] = {0, 0};
       int buf = 0;
       bool ok = true;
+      if (cres && !mbar_wait(cfull, 0, abort)) ok = false;
       for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
         const int Q = item / p.npairs, jp = item - Q * p.npairs;
         const int J0 = 2 * jp;
@@ -211,9 +236,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t sa = smem_u32(smem + stage * Cfg::kStage);
+          const uint32_t sa = smem_u32(smem + stage * stage_bytes);
           const uint32_t ahi = sa, alo = sa + 2 * kTileBytes;
-          const uint32_t chi = sa + Cfg::kABytes, clo = chi + Cfg::kCBytes;
+          const uint32_t chi = cres ? smem_u32(cbase + static_cast<size_t>(I) * 2 * Cfg::kCBytes) : sa + Cfg::kABytes;
+          const uint32_t clo = chi + Cfg::kCBytes;
           const bool mn = I > J0;
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
@@ -297,7 +323,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 struct SyrkParams {
   long kdim, kper;
   int npad2, ntile64, stages;
-  double* Kpart;
+  float* Kpart;  // fp32 partials: the TMEM accumulators stored as they are
   int* err;
 };
 
@@ -431,10 +457,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
         tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c0, v);
         const long cb = 2 * b + c0 / 64;
         if (diag && ra < cb) continue;  // upper-right sub-tile of a diagonal tile: its mirror is stored
-        double* out = p.Kpart + (s * p.ntile64 + tri_index(ra, cb)) * TILE2 + r * TILE + (c0 % 64);
+        float* out = p.Kpart + (s * p.ntile64 + tri_index(ra, cb)) * TILE2 + r * TILE + (c0 % 64);
 #pragma unroll
-        for (int j = 0; j < 16; j += 2)
-          *reinterpret_cast<double2*>(out + j) = make_double2(static_cast<double>(v[j]), static_cast<double>(v[j + 1]));
+        for (int j = 0; j < 16; j += 4) *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
       }
     } else if (lane == 0) {
       atomicOr(p.err, DEVERR_TIMEOUT);
@@ -491,12 +516,15 @@ int num_sms(int device) {
 template <int NOCCP>
 void launch_xform_tc(const CUtensorMap& mB, const CUtensorMap& mC, XformParams p, int device, cudaStream_t s) {
   using Cfg = XformCfg<NOCCP>;
-  p.stages = Cfg::stages();
-  size_t smem = Cfg::smem(p.stages);
-  static bool attr = false;
-  if (!attr) {
+  // keep C resident when it leaves room for at least 3 A stages
+  const int sr = Cfg::stages_resident(p.nt2);
+  p.c_resident = sr >= 3 ? 1 : 0;
+  p.stages = p.c_resident ? sr : Cfg::stages();
+  const size_t smem = p.c_resident ? Cfg::smem_resident(p.stages, p.nt2) : Cfg::smem(p.stages);
+  static size_t attr = 0;
+  if (smem > attr) {
     cudaFuncSetAttribute(k_xform_tc<NOCCP>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attr = true;
+    attr = smem;
   }
   int nitems = p.naux * p.npairs;
   int grid = std::min(nitems, num_sms(device));
@@ -566,8 +594,11 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   cudaStream_t s = ctx->stream;
   if ((rc = ensure(ctx, ctx->MOp, static_cast<size_t>(2 * noccp * npad2) * sizeof(__nv_bfloat16), "split C")) ||
       (rc = ensure(ctx, ctx->XT, static_cast<size_t>(2 * npad2) * kdim * sizeof(__nv_bfloat16), "split XT")) ||
-      (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(nsplit) * ntile2 * TILE2 * sizeof(double), "Kpart")))
+      (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(ntile2) * TILE2 * (sizeof(double) + nsplit * sizeof(float)),
+                   "Kpart")))  // fp64 sum area, then the fp32 split partials
     return rc;
+  double* Ksum = static_cast<double*>(ctx->Kpart.p);
+  float* Kpart32 = reinterpret_cast<float*>(Ksum + ntile2 * TILE2);
   __nv_bfloat16* Cmix = static_cast<__nv_bfloat16*>(ctx->MOp.p);
   __nv_bfloat16* XT = static_cast<__nv_bfloat16*>(ctx->XT.p);
   int launches = 0;
@@ -600,7 +631,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   sp.kper = kper;
   sp.npad2 = static_cast<int>(npad2);
   sp.ntile64 = static_cast<int>(ntile2);
-  sp.Kpart = static_cast<double*>(ctx->Kpart.p);
+  sp.Kpart = Kpart32;
   sp.err = static_cast<int*>(ctx->err.p);
   sp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
   size_t smem = static_cast<size_t>(sp.stages) * kSyStage + 1024 + 256;
@@ -613,8 +644,8 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   k_syrk_tc<<<grid, kTcThreads, smem, s>>>(mX, sp);
   ++launches;
   prof_mark(ctx, "syrk_tc");
-  launch_unpack_sym(static_cast<double*>(ctx->Kpart.p), nsplit, ntile2, n, dK, s);
-  ++launches;
+  launch_unpack_sym_f32(Kpart32, nsplit, ntile2, n, Ksum, dK, s);
+  launches += 2;
   prof_mark(ctx, "unpack_k");
   ctx->stats.kernels_last_fock = launches;
   return cuda_check(ctx, cudaGetLastError(), "mixed exchange launch");

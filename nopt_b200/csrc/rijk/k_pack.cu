@@ -52,6 +52,38 @@ __global__ void k_sum_splits(double* __restrict__ partial, int nsplit, long ntil
   }
 }
 
+// sum[idx] = sum_s partial[s][idx] for fp32 partials (the tcgen05 accumulators, exact in fp32),
+// summed in fp64; four consecutive elements per thread, four splits in flight.
+__global__ void k_sum_splits_f32(const float* __restrict__ partial, int nsplit, long ntile, double* __restrict__ sum) {
+  const long total4 = ntile * TILE2 / 4;
+  const float4* p4 = reinterpret_cast<const float4*>(partial);
+  for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total4;
+       i += static_cast<long>(gridDim.x) * blockDim.x) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int sp = 0;
+    for (; sp + 4 <= nsplit; sp += 4) {
+      float4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = p4[static_cast<long>(sp + u) * total4 + i];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        a0 += v[u].x;
+        a1 += v[u].y;
+        a2 += v[u].z;
+        a3 += v[u].w;
+      }
+    }
+    for (; sp < nsplit; ++sp) {
+      const float4 v = p4[static_cast<long>(sp) * total4 + i];
+      a0 += v.x;
+      a1 += v.y;
+      a2 += v.z;
+      a3 += v.w;
+    }
+    reinterpret_cast<double4*>(sum)[i] = make_double4(a0, a1, a2, a3);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_unpack_blocks(const double* __restrict__ packed, long n, long nb,
                                                       double* __restrict__ out) {
   __shared__ double blk[32][33];
@@ -104,6 +136,14 @@ void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* 
   if (nsplit > 1) k_sum_splits<<<grid_for(ntile * TILE2, 256), 256, 0, s>>>(p, nsplit, ntile);
   const long nb = (n + 31) / 32;
   k_unpack_blocks<<<static_cast<unsigned>(nb * nb), 256, 0, s>>>(p, n, nb, out);
+}
+
+// fp32 split partials -> their fp64 sum (into `sum`, ntile tiles) -> the full symmetric n x n matrix.
+void launch_unpack_sym_f32(const float* partial, int nsplit, long ntile, long n, double* sum, double* out,
+                           cudaStream_t s) {
+  k_sum_splits_f32<<<grid_for(ntile * TILE2 / 4, 256), 256, 0, s>>>(partial, nsplit, ntile, sum);
+  const long nb = (n + 31) / 32;
+  k_unpack_blocks<<<static_cast<unsigned>(nb * nb), 256, 0, s>>>(sum, n, nb, out);
 }
 
 void launch_scan_nonfinite(const double* x, long count, int* err, cudaStream_t s) {

@@ -110,6 +110,8 @@ int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& f
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s);
 void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s);
+void launch_unpack_sym_f32(const float* partial, int nsplit, long ntile, long n, double* sum, double* out,
+                           cudaStream_t s);
 void launch_scan_nonfinite(const double* x, long count, int* err, cudaStream_t s);
 
 // ---- k_metric.cu
