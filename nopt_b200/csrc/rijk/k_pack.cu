@@ -38,49 +38,48 @@ __global__ void k_pack_mo(const double* __restrict__ MO, long nocc, long n, long
   }
 }
 
-// Two steps: (1) sum the split partials into the first split's slot (each element read and
-// written by one thread, coalesced); (2) one CTA per 32 x 32 block of the full square copies
-// the stored tile block, transposing it through shared memory for the upper triangle.
-__global__ void k_sum_splits(double* __restrict__ partial, int nsplit, long ntile) {
-  const long total = ntile * TILE2;
-  const long sstride = total;
-  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  for (; idx < total; idx += static_cast<long>(gridDim.x) * blockDim.x) {
-    double v = partial[idx];
-    for (int s = 1; s < nsplit; ++s) v += partial[static_cast<long>(s) * sstride + idx];
-    partial[idx] = v;
+// Two steps: (1) sum the split partials (fp64, or the fp32 tcgen05 accumulators) into an fp64
+// packed buffer; (2) one CTA per 32 x 32 block of the full square copies the stored tile block,
+// transposing it through shared memory for the upper triangle.
+//
+// Step 1: a CTA owns 128 consecutive elements (32 lanes x 4); its 8 warps take every 8th split
+// each, four splits in flight, and the 8 warp sums are added in shared memory in warp order, so
+// the result does not depend on timing.  With out == partial (fp64) the sum overwrites split 0
+// after every warp has read it.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sum_splits(const T* partial, int nsplit, long total, double* out) {
+  __shared__ double red[8][32][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long e = (static_cast<long>(blockIdx.x) * 32 + lane) * 4;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  if (e < total) {
+    int sp = warp;
+    for (; sp + 24 < nsplit; sp += 32) {
+      T v[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[u][k] = partial[static_cast<long>(sp + 8 * u) * total + e + k];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a[k] += static_cast<double>(v[u][k]);
+    }
+    for (; sp < nsplit; sp += 8)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] += static_cast<double>(partial[static_cast<long>(sp) * total + e + k]);
   }
-}
-
-// sum[idx] = sum_s partial[s][idx] for fp32 partials (the tcgen05 accumulators, exact in fp32),
-// summed in fp64; four consecutive elements per thread, four splits in flight.
-__global__ void k_sum_splits_f32(const float* __restrict__ partial, int nsplit, long ntile, double* __restrict__ sum) {
-  const long total4 = ntile * TILE2 / 4;
-  const float4* p4 = reinterpret_cast<const float4*>(partial);
-  for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total4;
-       i += static_cast<long>(gridDim.x) * blockDim.x) {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int sp = 0;
-    for (; sp + 4 <= nsplit; sp += 4) {
-      float4 v[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = p4[static_cast<long>(sp + u) * total4 + i];
+  for (int k = 0; k < 4; ++k) red[warp][lane][k] = a[k];
+  __syncthreads();
+  if (warp == 0 && e < total) {
+    double r[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        a0 += v[u].x;
-        a1 += v[u].y;
-        a2 += v[u].z;
-        a3 += v[u].w;
-      }
+    for (int k = 0; k < 4; ++k) {
+      r[k] = red[0][lane][k];
+      for (int w = 1; w < 8; ++w) r[k] += red[w][lane][k];
     }
-    for (; sp < nsplit; ++sp) {
-      const float4 v = p4[static_cast<long>(sp) * total4 + i];
-      a0 += v.x;
-      a1 += v.y;
-      a2 += v.z;
-      a3 += v.w;
-    }
-    reinterpret_cast<double4*>(sum)[i] = make_double4(a0, a1, a2, a3);
+    *reinterpret_cast<double4*>(out + e) = make_double4(r[0], r[1], r[2], r[3]);
   }
 }
 
@@ -133,7 +132,8 @@ void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, 
 // Sums the split partials in place (into split 0) and writes the full symmetric n x n matrix.
 void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s) {
   double* p = partial;
-  if (nsplit > 1) k_sum_splits<<<grid_for(ntile * TILE2, 256), 256, 0, s>>>(p, nsplit, ntile);
+  const long total = ntile * TILE2;
+  if (nsplit > 1) k_sum_splits<double><<<static_cast<unsigned>((total + 127) / 128), 256, 0, s>>>(p, nsplit, total, p);
   const long nb = (n + 31) / 32;
   k_unpack_blocks<<<static_cast<unsigned>(nb * nb), 256, 0, s>>>(p, n, nb, out);
 }
@@ -141,7 +141,8 @@ void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* 
 // fp32 split partials -> their fp64 sum (into `sum`, ntile tiles) -> the full symmetric n x n matrix.
 void launch_unpack_sym_f32(const float* partial, int nsplit, long ntile, long n, double* sum, double* out,
                            cudaStream_t s) {
-  k_sum_splits_f32<<<grid_for(ntile * TILE2 / 4, 256), 256, 0, s>>>(partial, nsplit, ntile, sum);
+  const long total = ntile * TILE2;
+  k_sum_splits<float><<<static_cast<unsigned>((total + 127) / 128), 256, 0, s>>>(partial, nsplit, total, sum);
   const long nb = (n + 31) / 32;
   k_unpack_blocks<<<static_cast<unsigned>(nb * nb), 256, 0, s>>>(sum, n, nb, out);
 }
