@@ -32,9 +32,14 @@ import numpy as np  # noqa: E402
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernels,
 # from one ncu capture each (profiles/k_xform_f64_h2o16_dz.md, profiles/k_xform_tc_syrk_tc_h2o16_dz.md).
-NCU_TRAFFIC = {("h2o16_dz", "xform_f64"): 1.277519e9 + 0.439185e9,
-               ("h2o16_dz", "xform_tc"): 0.639804e9 + 0.199220e9,
-               ("h2o16_dz", "syrk_tc"): 0.228556e9 + 0.047133e9}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/fp64_exchange_h2o16_dz.md,
+# profiles/mixed_kernels_h2o16_dz.md)
+NCU_TRAFFIC = {("h2o16_dz", "xform_f64"): 1.277519e9 + 0.436856e9,
+               ("h2o16_dz", "syrk_f64"): 0.512381e9 + 0.021134e9,
+               ("h2o16_dz", "xform_tc"): 0.639340e9 + 0.201856e9,
+               ("h2o16_dz", "syrk_tc"): 0.228236e9 + 0.032031e9,
+               ("h2o16_dz", "coulomb_w_mixed"): 0.639341e9 + 0.004234e9,
+               ("h2o16_dz", "coulomb_j_mixed"): 0.638610e9 + 0.010762e9}
 WORKLOAD_NAMES = {"h2o6_dz": "(H2O)6 cc-pVDZ/cc-pVDZ-JKFIT", "h2o16_dz": "(H2O)16 cc-pVDZ/cc-pVDZ-JKFIT",
                   "c40h82_dz": "C40H82 cc-pVDZ/cc-pVDZ-JKFIT", "h2o32_tz": "(H2O)32 cc-pVTZ/cc-pVTZ-JKFIT"}
 METRIC = "RI-JK Fock builds/s (FP64 drop-in; mixed and SCF time beside it)"
@@ -403,6 +408,8 @@ def main():
                 bw = mbytes / (v * 1e-3) / 1e9
                 roofs[k] = {"bound": "hbm", "achieved": bw, "peak": hbm, "unit": "GB/s", "frac": bw / hbm,
                             "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        for k in roofs:
+            roofs[k]["traffic"] = NCU_TRAFFIC.get((args.workload, k))
         mixed["rooflines"] = roofs
         if mtop in roofs:
             mixed["roofline"] = dict(roofs[mtop], kernel=mtop)
