@@ -433,11 +433,14 @@ def main():
                 ("soscf_fp64", rijk.PREC_FP64, rijk.CONV_SOSCF),
                 ("soscf_mixed_then_fp64", rijk.PREC_MIXED, rijk.CONV_SOSCF))
         for name, prec, conv in runs:
-            torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
-            E, _, r = fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, conv_dm_rms=1e-10, guess=guess,
-                             converger=conv)
-            el = time.perf_counter() - t0
+            el = None
+            for _ in range(2):  # the faster of two runs: host-side latencies make single SCF timings noisy
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                E, _, r = fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, conv_dm_rms=1e-10, guess=guess,
+                                 converger=conv)
+                t = time.perf_counter() - t0
+                el = t if el is None else min(el, t)
             out[name] = {"seconds": el, "iterations": r["iterations"], "iterations_mixed": r["iterations_mixed"],
                          "energy": E, "ms_fock": r["ms_fock"], "ms_diag": r["ms_diag_phase"],
                          "converged": bool(r["converged"])}
@@ -448,6 +451,7 @@ def main():
         out["criterion"] = ("DIIS: density RMS change < 1e-10; SOSCF (the reference's converger): max|4 F_ai| < 1e-7 "
                             "or |dE| < 1e-10; mixed runs switch to FP64 when the DIIS error / max|4 F_ai| < 1e-5")
         out["start"] = "superposition of atomic densities (%.2f s on the host, not in the SCF time)" % t_guess
+        out["timing"] = "wall time of rijk_scf, the faster of two runs"
         scf = out
 
     cpu = None
