@@ -473,6 +473,175 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
   }
 }
 
+// --------------------------------------------------- K4 on CTA pairs: SYRK ----
+// 256 x 256 output tiles on a pair of CTAs (cluster of 2) with tcgen05.mma.cta_group::2: CTA r
+// holds rows 128 r .. 128 r + 127 of the tile's A panel and of its B panel (the same 64 KB
+// stage layout as k_syrk_tc) and rows 128 r .. of the accumulator in its TMEM; the leader
+// (rank 0) issues M = 256, N = 256 MMAs over both CTAs' shared memory.  Each operand byte
+// crosses L2 -> SM once for twice the FLOPs of a 128 x 128 tile.  Both CTAs' TMA loads complete
+// on the leader's stage barrier, which alone expects the pair's bytes; the leader's commits
+// release the stage (and signal the accumulator) in both CTAs.  A last 256-row panel that
+// runs past npad2 computes rows and columns that are never stored.
+struct SyrkPairParams {
+  long kdim, kper;
+  int npad2, nt2, ntile64, stages;
+  float* Kpart;
+  int* err;
+};
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constant__ CUtensorMap mapX, SyrkPairParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  const int S = p.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * kSyStage);
+  uint64_t* empty = full + S;
+  uint64_t* tfull = empty + S;
+  uint64_t* drain = tfull + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  long a, b;
+  tri_decode(blockIdx.x / 2, a, b);  // 256-row panels, b <= a
+  const bool diag = a == b;
+  const long s = blockIdx.y;
+  const long k0 = s * p.kper;
+  const long k1 = std::min(k0 + p.kper, p.kdim);
+  const int nch = static_cast<int>((k1 - k0 + 63) / 64);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(tfull, 1);
+    mbar_init(drain, 1);
+    *abort = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(tmem_slot, 256);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // both CTAs' barriers and TMEM exist before any traffic between them
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      tma_prefetch_desc(&mapX);
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      const uint32_t cta_bytes = diag ? 2 * kSyOpBytes : 4 * kSyOpBytes;
+      const int ra = static_cast<int>(a * 256 + rank * 128), rb = static_cast<int>(b * 256 + rank * 128);
+      for (int c = 0; c < nch; ++c) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, abort)) {
+          ok = false;
+          break;
+        }
+        uint8_t* st = smem + stage * kSyStage;
+        const int x = static_cast<int>(k0 + 64L * c);
+        if (leader) mbar_expect_tx(&full[stage], 2 * cta_bytes);  // this CTA's bytes and the peer's
+        tma_load_2d_pair(st, &mapX, &full[stage], x, ra);                                 // A hi
+        tma_load_2d_pair(st + kSyOpBytes, &mapX, &full[stage], x, p.npad2 + ra);          // A lo
+        if (!diag) {
+          tma_load_2d_pair(st + 2 * kSyOpBytes, &mapX, &full[stage], x, rb);              // B hi
+          tma_load_2d_pair(st + 3 * kSyOpBytes, &mapX, &full[stage], x, p.npad2 + rb);    // B lo
+        }
+        if (++stage == S) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      if (!ok) {
+        *abort = 1;
+        atomicOr(p.err, DEVERR_TIMEOUT);
+      }
+      if (leader) {  // every issued load of the pair has landed before the pair may exit
+        volatile int never = 0;
+        for (int i = 0; i < S; ++i) {
+          uint32_t par = (i < stage) ? phase : (phase ^ 1);
+          mbar_wait(&full[i], par, &never);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (leader && lane == 0) {
+      constexpr uint64_t kKdesc = sw128_desc_bits(16, 1024);
+      constexpr uint32_t id = idesc_bf16_f32(256, 256, 0, 0);
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      for (int c = 0; c < nch; ++c) {
+        if (!mbar_wait(&full[stage], phase, abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + stage * kSyStage);
+        const uint32_t ah = sa, al = sa + kSyOpBytes;
+        const uint32_t bh = diag ? ah : sa + 2 * kSyOpBytes, bl = diag ? al : sa + 3 * kSyOpBytes;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const uint64_t dah = sw128_desc(ah + kk * 32, kKdesc), dal = sw128_desc(al + kk * 32, kKdesc);
+          const uint64_t dbh = sw128_desc(bh + kk * 32, kKdesc), dbl = sw128_desc(bl + kk * 32, kKdesc);
+          umma_bf16_pair(tmem, dah, dbh, id, (c | kk) != 0 ? 1u : 0u);
+          umma_bf16_pair(tmem, dah, dbl, id, 1u);
+          umma_bf16_pair(tmem, dal, dbh, id, 1u);
+        }
+        umma_commit_pair(&empty[stage], 0x3);
+        if (++stage == S) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      if (!ok) {
+        *abort = 1;
+        atomicOr(p.err, DEVERR_TIMEOUT);
+      }
+      umma_commit_pair(tfull, 0x3);
+      umma_commit_pair(drain, 0x3);
+    }
+  } else {
+    const int q = warp & 3;
+    if (mbar_wait(tfull, 0, abort) && !*abort) {
+      tc_fence_after();
+      const long row = a * 256 + rank * 128 + q * 32 + lane;  // row of K
+      const long ra = row / 64;
+      const int r = static_cast<int>(row % 64);
+#pragma unroll 1
+      for (int c0 = 0; c0 < 256; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c0, v);
+        const long cb = (b * 256 + c0) / 64;
+        if (ra < cb || ra >= p.nt2 || cb >= p.nt2) continue;  // upper triangle, or past npad2
+        float* out = p.Kpart + (s * p.ntile64 + tri_index(ra, cb)) * TILE2 + r * TILE + (c0 % 64);
+#pragma unroll
+        for (int j = 0; j < 16; j += 4) *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+      }
+    } else if (lane == 0) {
+      atomicOr(p.err, DEVERR_TIMEOUT);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1 && lane == 0) {  // no MMA of the pair still writes this CTA's TMEM
+    volatile int never = 0;
+    if (!mbar_wait(drain, 0, &never)) atomicOr(p.err, DEVERR_TIMEOUT);
+  }
+  __syncthreads();
+  cluster_sync_all();  // neither CTA frees its TMEM or exits while the pair's work may touch it
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem, 256);
+  }
+}
+
 // ------------------------------------------------------------- tensor maps ----
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -591,10 +760,30 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   const long per = std::max<long>(2, (nchunks + best - 1) / best);
   const long kper = per * 64;
   const int nsplit = static_cast<int>((kdim + kper - 1) / kper);
+  // K on CTA pairs with 256 x 256 tiles once npad2 >= 1024 (at most one half-empty panel, <= 12.5 %
+  // wasted); its split count fills whole waves of SM pairs the same way
+  const bool pair_syrk = npad2 >= 1024;
+  const long nb256 = (npad2 + 255) / 256, tiles256 = nb256 * (nb256 + 1) / 2, pairs = sms / 2;
+  long best2 = std::max<long>(1, (4L * pairs + tiles256 - 1) / tiles256);
+  {
+    const long want2 = best2;
+    double eff2 = 0.0;
+    for (long sp = want2; sp <= 4 * want2 && sp <= std::max<long>(1, nchunks / 2); ++sp) {
+      const long n2 = tiles256 * sp, waves = (n2 + pairs - 1) / pairs;
+      const double eff = static_cast<double>(n2) / static_cast<double>(waves * pairs);
+      if (eff > eff2 + 0.02) {
+        eff2 = eff;
+        best2 = sp;
+      }
+    }
+  }
+  const long kper2 = std::max<long>(2, (nchunks + best2 - 1) / best2) * 64;
+  const int nsplit2 = static_cast<int>((kdim + kper2 - 1) / kper2);
+  const int nsplit_k = pair_syrk ? nsplit2 : nsplit;
   cudaStream_t s = ctx->stream;
   if ((rc = ensure(ctx, ctx->MOp, static_cast<size_t>(2 * noccp * npad2) * sizeof(__nv_bfloat16), "split C")) ||
       (rc = ensure(ctx, ctx->XT, static_cast<size_t>(2 * npad2) * kdim * sizeof(__nv_bfloat16), "split XT")) ||
-      (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(ntile2) * TILE2 * (sizeof(double) + nsplit * sizeof(float)),
+      (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(ntile2) * TILE2 * (sizeof(double) + nsplit_k * sizeof(float)),
                    "Kpart")))  // fp64 sum area, then the fp32 split partials
     return rc;
   double* Ksum = static_cast<double*>(ctx->Kpart.p);
@@ -626,6 +815,44 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   kXformTable[noccp / 16](mB, mC, xp, ctx->device, s);
   ++launches;
   prof_mark(ctx, "xform_tc");
+  if (pair_syrk) {
+    SyrkPairParams pp{};
+    pp.kdim = kdim;
+    pp.kper = kper2;
+    pp.npad2 = static_cast<int>(npad2);
+    pp.nt2 = static_cast<int>(nt2);
+    pp.ntile64 = static_cast<int>(ntile2);
+    pp.Kpart = Kpart32;
+    pp.err = static_cast<int*>(ctx->err.p);
+    pp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
+    const size_t smem2 = static_cast<size_t>(pp.stages) * kSyStage + 1024 + 256;
+    static bool attr2 = false;
+    if (!attr2) {
+      cudaFuncSetAttribute(k_syrk_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem2));
+      attr2 = true;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(2 * tiles256), static_cast<unsigned>(nsplit2));
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = smem2;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    rc = cuda_check(ctx, cudaLaunchKernelEx(&cfg, k_syrk_tc2, mX, pp), "CTA-pair SYRK launch");
+    if (rc) return rc;
+    ++launches;
+    prof_mark(ctx, "syrk_tc");
+    launch_unpack_sym_f32(Kpart32, nsplit2, ntile2, n, Ksum, dK, s);
+    launches += 2;
+    prof_mark(ctx, "unpack_k");
+    ctx->stats.kernels_last_fock = launches;
+    return cuda_check(ctx, cudaGetLastError(), "mixed exchange launch");
+  }
   SyrkParams sp{};
   sp.kdim = kdim;
   sp.kper = kper;
