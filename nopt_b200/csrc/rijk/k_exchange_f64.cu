@@ -194,11 +194,31 @@ __global__ void __launch_bounds__(S_THREADS)
   }
 }
 
-// Splits of the contraction range: enough CTAs for about two waves of the 2 CTAs per SM the
-// kernel fits (shared memory), chosen among [s_min, 4 s_min] so the last wave is fullest.
+namespace {
+constexpr size_t kSyrkSmem = 4 * 64 * LDK * sizeof(double);
+
+// CTAs of k_syrk_f64 resident per SM (registers and shared memory), from the runtime.
+int syrk_ctas_per_sm() {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaFuncSetAttribute(k_syrk_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSyrkSmem));
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_syrk_f64, S_THREADS, kSyrkSmem) != cudaSuccess || nb < 1)
+      nb = 2;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    per_sm = nb * sms;  // slots of one wave
+  }
+  return per_sm;
+}
+}  // namespace
+
+// Splits of the contraction range: enough CTAs for about two waves of the kernel's resident
+// slots (CTAs per SM x SMs), chosen among [s_min, 4 s_min] so the last wave is fullest.
 int syrk_nsplit(long nt, long kdim) {
   const long ntile = nt * (nt + 1) / 2;
-  const long slots = 148L * 2;
+  const long slots = syrk_ctas_per_sm();
   const long maxs = std::max<long>(1, kdim / (KC * 8));
   const long need = slots * 19 / 10;
   const long smin = std::min(maxs, std::max<long>(1, (need + ntile - 1) / ntile));
@@ -221,13 +241,8 @@ void launch_syrk_f64(const double* XT, long npad, long nt, long kdim, int nsplit
   long ntile = nt * (nt + 1) / 2;
   long kper = round_up((kdim + nsplit - 1) / nsplit, KC);
   dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(nsplit));
-  const size_t smem = 4 * 64 * LDK * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_syrk_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attr = true;
-  }
-  k_syrk_f64<<<grid, S_THREADS, smem, s>>>(XT, kdim, kper, ntile, Kpart);
+  syrk_ctas_per_sm();  // sets the shared-memory attribute once
+  k_syrk_f64<<<grid, S_THREADS, kSyrkSmem, s>>>(XT, kdim, kper, ntile, Kpart);
 }
 
 }  // namespace rijk
