@@ -131,7 +131,7 @@ static void prof_collect(rijk_ctx* ctx) {
 }
 
 int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
-                     int precision) {
+                     int precision, cudaEvent_t mo_ready, cudaEvent_t j_done) {
   // naux here is the number of aux functions this context holds (a slice under rijk_set_aux_range)
   const long n = ctx->n, naux = ctx->nq, nt = ctx->nt, npad = ctx->npad, ntile = ctx->ntile;
   const long tile_elems = ntile * TILE2;
@@ -170,6 +170,8 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
   prof_mark(ctx, "unpack_j");
   launches += (precision == RIJK_PREC_MIXED ? 5 : 4) + (nsJ > 1 ? 1 : 0);  // pack, w (+ chunk sum), j, unpack (+ split sum)
   cudaEventRecord(ctx->ev1, s);
+  if (j_done) cudaEventRecord(j_done, s);
+  if (mo_ready && nocc > 0) cudaStreamWaitEvent(s, mo_ready, 0);
 
   if (nocc == 0) {
     cudaMemsetAsync(dK, 0, n * n * sizeof(double), s);
@@ -232,6 +234,12 @@ RIJK_API int rijk_create(rijk_ctx** out, int device) {
     return RIJK_ERR_CUDA;
   }
   ctx->own_stream = true;
+  if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    rijk_destroy(ctx);
+    return RIJK_ERR_CUDA;
+  }
+  cudaEventCreateWithFlags(&ctx->ev_mo, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ctx->ev_j, cudaEventDisableTiming);
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
   cudaEventCreate(&ctx->ev2);
@@ -260,7 +268,11 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
   for (DeviceBuf* b : bufs) release(*b);
   if (ctx->cublas) cublasDestroy(ctx->cublas);
   if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
-  cudaEvent_t evs[] = {ctx->ev0, ctx->ev1, ctx->ev2, ctx->ev3};
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
+  cudaEvent_t evs[] = {ctx->ev0, ctx->ev1, ctx->ev2, ctx->ev3, ctx->ev_mo, ctx->ev_j};
   for (cudaEvent_t ev : evs)
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : ctx->pev)
@@ -588,18 +600,30 @@ RIJK_API int rijk_fock(rijk_ctx* ctx, const double* D, const double* MO, long no
       (rc = ensure(ctx, ctx->stageK, nn, "stage K")) ||
       (rc = ensure(ctx, ctx->stageMO, std::max<size_t>(1, nocc * n * sizeof(double)), "stage MO")))
     return rc;
-  cudaStream_t s = ctx->stream;
+  cudaStream_t s = ctx->stream, c = ctx->copy_stream;
+  // D on the build's stream; the orbitals on the copy stream (the Coulomb passes do not need
+  // them); J comes down on the copy stream while the exchange runs; K on the build's stream.
+  // Both staging areas are free: the previous call ended with both streams synchronised.
   rc = cuda_check(ctx, cudaMemcpyAsync(ctx->stageD.p, D, nn, cudaMemcpyHostToDevice, s), "H2D D");
-  if (!rc && nocc > 0)
-    rc = cuda_check(ctx, cudaMemcpyAsync(ctx->stageMO.p, MO, nocc * n * sizeof(double), cudaMemcpyHostToDevice, s),
+  if (!rc && nocc > 0) {
+    rc = cuda_check(ctx, cudaMemcpyAsync(ctx->stageMO.p, MO, nocc * n * sizeof(double), cudaMemcpyHostToDevice, c),
                     "H2D MO");
+    if (!rc) cudaEventRecord(ctx->ev_mo, c);
+  }
   if (rc) return rc;
   rc = fock_device_impl(ctx, static_cast<const double*>(ctx->stageD.p), static_cast<const double*>(ctx->stageMO.p),
-                        nocc, static_cast<double*>(ctx->stageJ.p), static_cast<double*>(ctx->stageK.p), precision);
-  if (rc) return rc;
-  rc = cuda_check(ctx, cudaMemcpyAsync(J, ctx->stageJ.p, nn, cudaMemcpyDeviceToHost, s), "D2H J");
+                        nocc, static_cast<double*>(ctx->stageJ.p), static_cast<double*>(ctx->stageK.p), precision,
+                        nocc > 0 ? ctx->ev_mo : nullptr, ctx->ev_j);
+  if (rc) {
+    cudaStreamSynchronize(c);
+    return rc;
+  }
+  cudaStreamWaitEvent(c, ctx->ev_j, 0);
+  rc = cuda_check(ctx, cudaMemcpyAsync(J, ctx->stageJ.p, nn, cudaMemcpyDeviceToHost, c), "D2H J");
   if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(K, ctx->stageK.p, nn, cudaMemcpyDeviceToHost, s), "D2H K");
+  const int rc_c = cuda_check(ctx, cudaStreamSynchronize(c), "rijk_fock copies");
   if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_fock");
+  if (!rc) rc = rc_c;
   if (!rc) rc = check_device_error(ctx);
   if (rc) return rc;
   ctx->stats.ms_coulomb = elapsed(ctx->ev0, ctx->ev1);

@@ -50,6 +50,10 @@ struct rijk_ctx {
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+  // host-pointer builds (rijk_fock): the orbitals go up and J comes down on a second stream while
+  // the Coulomb and exchange kernels run
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_mo = nullptr, ev_j = nullptr;
 
   long n = 0, naux = 0, npad = 0, nt = 0, ntile = 0;
   long q0 = 0, nq = 0;  // aux functions [q0, q0 + nq) held in B (all of them unless rijk_set_aux_range)
@@ -94,9 +98,11 @@ void release(DeviceBuf& b);
 float elapsed(cudaEvent_t a, cudaEvent_t b);
 int check_device_error(rijk_ctx* ctx);
 int check_fock_args(rijk_ctx* ctx, long nocc, int precision);
-// One Fock build on device pointers (J into dJ, K into dK), asynchronous on ctx->stream.
+// One Fock build on device pointers (J into dJ, K into dK), asynchronous on ctx->stream.  With
+// mo_ready the exchange waits for that event (dMO is written on another stream); with j_done the
+// event is recorded once J is complete, before the exchange kernels.
 int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long nocc, double* dJ, double* dK,
-                     int precision);
+                     int precision, cudaEvent_t mo_ready = nullptr, cudaEvent_t j_done = nullptr);
 // Metric factor from (P|Q) held in host memory (cudaMemcpyHostToDevice) or device memory.
 int set_metric_impl(rijk_ctx* ctx, const double* PQ, cudaMemcpyKind kind, long naux, int form);
 // Fitted tensor from three-centre integrals that `fill` writes, one block of tile rows at a time:
