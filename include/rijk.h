@@ -78,6 +78,7 @@ typedef struct {
   double ms_setup_ints;   /* last rijk_set_basis: device time of the integral kernels          */
   int kernels_setup_ints; /* integral kernels it launched                                    */
   long q0, nq;            /* aux functions [q0, q0 + nq) held (all of them unless sliced)      */
+  long grad_qchunk;       /* aux functions per chunk of the last rijk_grad (naux: one chunk)    */
 } rijk_stats_t;
 
 int rijk_create(rijk_ctx** ctx, int device);
@@ -261,6 +262,11 @@ int rijk_mo_ints_aaag(rijk_ctx* ctx, double* MO_INTS, const double* MO_VEC, long
  * arguments are never written by it and have no counterpart here.) */
 int rijk_soscf_hess_ints(rijk_ctx* ctx, double* aa_J, double* aa_K, const double* MO_VEC, long n_c, long n_a,
                          long n_mo);
+
+/* Aux functions per chunk of rijk_grad's Gamma stage (0, the default: all of them when HBM holds
+ * Gamma for every aux function, else as many as it holds).  Below naux, each chunk's
+ * half-transformed tensor is recomputed in tiles instead of read from the stored one. */
+int rijk_set_grad_chunk(rijk_ctx* ctx, long q_per_chunk);
 
 /* Adjoint of the Fock build (no reference counterpart; the reference differentiates by finite
  * differences, src/QM_calc.cpp:142).  For the orbitals MO (n_c rows of n, host) and D = C^T C:

@@ -50,6 +50,22 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Compensated (Neumaier) summation: the pair (s, c) carries the sum, c collecting the rounding
+// error of every addition (Neumaier, Z. Angew. Math. Mech. 54 (1974) 39).  Used for the energy.
+__host__ __device__ __forceinline__ void neumaier_add(double& s, double& c, double x) {
+  const double t = s + x;
+  c += (fabs(s) >= fabs(x)) ? (s - t) + x : (x - t) + s;
+  s = t;
+}
+__device__ __forceinline__ void warp_sum_comp(double& s, double& c) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double os = __shfl_xor_sync(0xffffffffu, s, o), oc = __shfl_xor_sync(0xffffffffu, c, o);
+    neumaier_add(s, c, os);
+    c += oc;
+  }
+}
+
 // Tile (I, J), I >= J, of the lower block triangle.
 __host__ __device__ __forceinline__ long tri_index(long I, long J) { return I * (I + 1) / 2 + J; }
 

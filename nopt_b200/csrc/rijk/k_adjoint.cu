@@ -15,10 +15,13 @@
 // (E depends on the metric only through V^-1 = M^T M, for either metric form).
 //
 // Device work, FP64 throughout: one FP64 Fock build (which leaves w and the half-transformed
-// XT in the context), then per Q the small products Y^Q = X^Q C^T and T^Q = Y^Q C (cuBLAS
-// strided-batched DGEMM), then k_gamma_f64 forms the packed Gamma tiles
-// Gamma^Q_tile = 4 w_Q D_tile - 2 T^Q_rows T^Q... with DMMA, and two plain DGEMMs contract
-// Gamma with M (raw three-centre gradient) and with B (metric gradient).
+// XT in the context), then, over chunks of aux functions, the small products Y^Q = X^Q C^T and
+// T^Q = Y^Q C (cuBLAS strided-batched DGEMM), k_gamma_f64 forming the packed Gamma tiles
+// Gamma^Q_tile = 4 w_Q D_tile - 2 T^Q_rows Ct_cols^T with DMMA, and two DGEMMs contracting the
+// chunk of Gamma with M (raw three-centre gradient, accumulated) and with B (its rows of G, the
+// metric gradient).  When HBM cannot hold Gamma for every aux function at once, each chunk's
+// X^Q is recomputed in tiles from B instead of read from the stored tensor.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -138,19 +141,27 @@ __global__ void k_fock_sym(const double* __restrict__ H, const double* __restric
   for (; idx < nn; idx += static_cast<long>(gridDim.x) * blockDim.x) F[idx] = H[idx] + 2.0 * J[idx] - K[idx];
 }
 
+// partial[b], partial[512 + b]: compensated sum of D (F + H) over a grid-stride slice
 __global__ void k_energy_partial(const double* __restrict__ D, const double* __restrict__ F,
                                  const double* __restrict__ H, long nn, double* __restrict__ partial) {
-  double acc = 0.0;
+  double s = 0.0, c = 0.0;
   for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < nn; i += static_cast<long>(gridDim.x) * blockDim.x)
-    acc += D[i] * (F[i] + H[i]);
-  acc = warp_sum(acc);
-  __shared__ double sh[8];
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    neumaier_add(s, c, D[i] * (F[i] + H[i]));
+  warp_sum_comp(s, c);
+  __shared__ double sh[2][8];
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = s;
+    sh[1][threadIdx.x >> 5] = c;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int i = 0; i < 8; ++i) s += sh[i];
-    partial[blockIdx.x] = s;
+    double t = 0.0, u = 0.0;
+    for (int i = 0; i < 8; ++i) {
+      neumaier_add(t, u, sh[0][i]);
+      u += sh[1][i];
+    }
+    partial[blockIdx.x] = t;
+    partial[512 + blockIdx.x] = u;
   }
 }
 
@@ -164,6 +175,13 @@ unsigned grid_of(long total) {
 }  // namespace rijk
 
 using namespace rijk;
+
+RIJK_API int rijk_set_grad_chunk(rijk_ctx* ctx, long q_per_chunk) {
+  if (!ctx) return RIJK_ERR_ARG;
+  if (q_per_chunk < 0) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_grad_chunk: negative chunk");
+  ctx->grad_qchunk = q_per_chunk;
+  return RIJK_OK;
+}
 
 RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double* H, double e_nuc, double* E,
                        double* dEdC, double* dEdI3, double* dEdPQ) {
@@ -195,7 +213,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
       (rc = chk(ensure(ctx, dD, b_nn, "grad D"))) || (rc = chk(ensure(ctx, dJ, b_nn, "grad J"))) ||
       (rc = chk(ensure(ctx, dK, b_nn, "grad K"))) || (rc = chk(ensure(ctx, dF, b_nn, "grad F"))) ||
       (rc = chk(ensure(ctx, dG, nocc * n * sizeof(double), "grad dEdC"))) ||
-      (rc = chk(ensure(ctx, red, 512 * sizeof(double), "grad reduce"))))
+      (rc = chk(ensure(ctx, red, 1024 * sizeof(double), "grad reduce"))))
     return rc;
   double* pMO = static_cast<double*>(dMO.p);
   double* pD = static_cast<double*>(dD.p);
@@ -213,81 +231,120 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   // dE/dC = 4 C F  (column-major n x n_c = 4 F Mt)
   const double four = 4.0;
   cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nci, ni, &four, pF, ni, pMO, ni, &zero, static_cast<double*>(dG.p), ni);
-  std::vector<double> part(512);
-  cudaMemcpyAsync(part.data(), red.p, 512 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  std::vector<double> part(1024);
+  cudaMemcpyAsync(part.data(), red.p, 1024 * sizeof(double), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(dEdC, dG.p, nocc * n * sizeof(double), cudaMemcpyDeviceToHost, s);
   if ((rc = chk(cuda_check(ctx, cudaStreamSynchronize(s), "rijk_grad energy"))) || (rc = chk(check_device_error(ctx))))
     return rc;
-  double e = e_nuc;
-  for (double v : part) e += v;
-  *E = e;
+  double es = 0.0, ec = 0.0;  // compensated: the 512 block sums, their compensations, then e_nuc
+  for (int b = 0; b < 512; ++b) {
+    neumaier_add(es, ec, part[b]);
+    ec += part[512 + b];
+  }
+  neumaier_add(es, ec, e_nuc);
+  *E = es + ec;
   if (!dEdI3 && !dEdPQ) {
     cleanup();
     return RIJK_OK;
   }
-  // per-Q small products over the half-transformed tensor XT[nu][Q*noccp + i] of the FP64 build
+  // Gamma and its contractions over chunks of aux functions [q0, q0 + qc).  X^Q comes from the
+  // tensor the FP64 build left in HBM when every chunk fits at once; otherwise (HBM short, or a
+  // chunk size set by rijk_set_grad_chunk) each chunk's X^Q is recomputed in tiles by the
+  // half-transform kernel, and only one chunk of X, Y, T and Gamma exists at a time.
   const long kdim = naux * noccp;
-  if ((rc = chk(ensure(ctx, Y, static_cast<size_t>(naux) * noccp * noccp * sizeof(double), "grad Y"))) ||
-      (rc = chk(ensure(ctx, Tb, static_cast<size_t>(naux) * npad * noccp * sizeof(double), "grad T"))) ||
-      (rc = chk(ensure(ctx, Ct, static_cast<size_t>(npad) * noccp * sizeof(double), "grad Ct"))) ||
-      (rc = chk(ensure(ctx, Gam, static_cast<size_t>(naux) * te * sizeof(double), "grad Gamma"))))
-    return rc;
-  const double* XT = static_cast<const double*>(ctx->XT.p);
   const double* MOp = static_cast<const double*>(ctx->MOp.p);
-  const int ncp = static_cast<int>(noccp), npi = static_cast<int>(npad);
-  // Y^Q (noccp x noccp) = X^Q (noccp x npad, column-major view of XT, ld kdim) . Cm (npad x noccp)
-  cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, ncp, ncp, npi, &one, XT, static_cast<int>(kdim), noccp, MOp,
-                            npi, 0, &zero, static_cast<double*>(Y.p), ncp, noccp * noccp, static_cast<int>(naux));
-  // T^Q as [mu][i] = (Y^Q C) column-major (noccp x npad): Y^Q (noccp x noccp) . Cm^T
-  cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_T, ncp, npi, ncp, &one, static_cast<const double*>(Y.p), ncp,
-                            noccp * noccp, MOp, npi, 0, &zero, static_cast<double*>(Tb.p), ncp, npad * noccp,
-                            static_cast<int>(naux));
-  k_transpose_mo<<<grid_of(noccp * npad), 256, 0, s>>>(MOp, noccp, npad, static_cast<double*>(Ct.p));
-  {
-    const size_t smem = 4 * 64 * LDK * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_gamma_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-      attr = true;
-    }
-    dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(naux));
-    k_gamma_f64<<<grid, G_THREADS, smem, s>>>(static_cast<const double*>(Tb.p), static_cast<const double*>(Ct.p), pD,
-                                              static_cast<const double*>(ctx->w.p), n, npad, noccp, te,
-                                              static_cast<double*>(Gam.p));
-  }
-  release(Y);
-  release(Tb);
-  double* pGam = static_cast<double*>(Gam.p);
   const double* pM = static_cast<const double*>(ctx->M.p);  // row-major [Q][P], ld nauxp
   const int na = static_cast<int>(naux), nap = static_cast<int>(nauxp), tei = static_cast<int>(te);
+  const int ncp = static_cast<int>(noccp), npi = static_cast<int>(npad);
+  if (dEdI3 && ((rc = chk(ensure(ctx, R, static_cast<size_t>(te) * naux * sizeof(double), "grad R"))) ||
+                (rc = chk(ensure(ctx, out, static_cast<size_t>(n * (n + 1) / 2) * naux * sizeof(double), "grad dI3")))))
+    return rc;
+  if (dEdPQ && ((rc = chk(ensure(ctx, Gm, static_cast<size_t>(naux) * naux * sizeof(double), "grad G"))) ||
+                (rc = chk(ensure(ctx, T1, static_cast<size_t>(naux) * naux * sizeof(double), "grad T1")))))
+    return rc;
+  if ((rc = chk(ensure(ctx, Ct, static_cast<size_t>(npad) * noccp * sizeof(double), "grad Ct")))) return rc;
+  k_transpose_mo<<<grid_of(noccp * npad), 256, 0, s>>>(MOp, noccp, npad, static_cast<double*>(Ct.p));
+  // bytes per aux function of one chunk: Y, T, Gamma (and X when recomputed)
+  const double per_q = 8.0 * (static_cast<double>(noccp) * noccp + static_cast<double>(npad) * noccp + te);
+  const double per_q_x = per_q + 8.0 * npad * noccp;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const double room = 0.85 * static_cast<double>(free_b) - 64.0 * 1024 * 1024;
+  long qc = ctx->grad_qchunk > 0 ? std::min(ctx->grad_qchunk, naux) : naux;
+  if (ctx->grad_qchunk <= 0 && per_q * naux > room)
+    qc = std::max<long>(1, std::min<long>(naux, static_cast<long>(room / per_q_x)));
+  const bool recompute = qc < naux;
+  if ((rc = chk(ensure(ctx, Y, static_cast<size_t>(qc) * noccp * noccp * sizeof(double), "grad Y"))) ||
+      (rc = chk(ensure(ctx, Tb, static_cast<size_t>(qc) * npad * noccp * sizeof(double), "grad T"))) ||
+      (rc = chk(ensure(ctx, Gam, static_cast<size_t>(qc) * te * sizeof(double), "grad Gamma"))))
+    return rc;
+  DeviceBuf Xc;
+  if (recompute && (rc = chk(ensure(ctx, Xc, static_cast<size_t>(npad) * qc * noccp * sizeof(double), "grad X chunk")))) {
+    release(Xc);
+    return rc;
+  }
+  double* pGam = static_cast<double*>(Gam.p);
+  const size_t gsmem = 4 * 64 * LDK * sizeof(double);
+  static bool gattr = false;
+  if (!gattr) {
+    cudaFuncSetAttribute(k_gamma_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(gsmem));
+    gattr = true;
+  }
+  const double half = 0.5;
+  for (long q0 = 0; q0 < naux; q0 += qc) {
+    const long nq = std::min(qc, naux - q0);
+    const int nqi = static_cast<int>(nq);
+    const double* X;  // X^Q_{i nu} at X[nu * ldx + (Q - q0) * noccp + i]
+    long ldx;
+    if (recompute) {
+      launch_xform_f64(static_cast<const double*>(ctx->B.p) + q0 * te, MOp, nq, nt, noccp, static_cast<double*>(Xc.p), s);
+      X = static_cast<const double*>(Xc.p);
+      ldx = nq * noccp;
+    } else {
+      X = static_cast<const double*>(ctx->XT.p) + q0 * noccp;
+      ldx = kdim;
+    }
+    // Y^Q (noccp x noccp) = X^Q (noccp x npad, column-major view, ld ldx) . Cm (npad x noccp)
+    cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, ncp, ncp, npi, &one, X, static_cast<int>(ldx), noccp, MOp,
+                              npi, 0, &zero, static_cast<double*>(Y.p), ncp, noccp * noccp, nqi);
+    // T^Q as [mu][i] = (Y^Q C) column-major (noccp x npad): Y^Q (noccp x noccp) . Cm^T
+    cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_T, ncp, npi, ncp, &one, static_cast<const double*>(Y.p), ncp,
+                              noccp * noccp, MOp, npi, 0, &zero, static_cast<double*>(Tb.p), ncp, npad * noccp, nqi);
+    dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(nq));
+    k_gamma_f64<<<grid, G_THREADS, gsmem, s>>>(static_cast<const double*>(Tb.p), static_cast<const double*>(Ct.p), pD,
+                                               static_cast<const double*>(ctx->w.p) + q0, n, npad, noccp, te, pGam);
+    if (dEdI3) {
+      // R (te x naux, column-major) += Gamma_chunk_cm (te x nq) . (rows q0.. of M, as nq x naux)
+      const double beta = q0 == 0 ? 0.0 : 1.0;
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, tei, na, nqi, &one, pGam, tei, pM + q0 * nauxp, nap, &beta,
+                  static_cast<double*>(R.p), tei);
+    }
+    if (dEdPQ) {
+      // rows q0.. of G = 1/2 sum_e omega_e Gamma[Q][e] B[R][e] (omega = 2 off-diagonal tiles)
+      k_scale_offdiag<<<grid_of(nq * te), 256, 0, s>>>(pGam, nq, ntile, 2.0, 1.0);
+      cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nqi, na, tei, &half, pGam, tei, static_cast<const double*>(ctx->B.p),
+                  tei, &zero, static_cast<double*>(Gm.p) + q0, na);
+    }
+  }
+  release(Xc);
+  release(Y);
+  release(Tb);
   if (dEdI3) {
-    // R (te x naux, column-major) = Gamma_cm (te x naux) . M_cm^T, M_cm(P, Q) = M[Q][P]
-    if ((rc = chk(ensure(ctx, R, static_cast<size_t>(te) * naux * sizeof(double), "grad R"))) ||
-        (rc = chk(ensure(ctx, out, static_cast<size_t>(n * (n + 1) / 2) * naux * sizeof(double), "grad dI3"))))
-      return rc;
-    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, tei, na, na, &one, pGam, tei, pM, nap, &zero, static_cast<double*>(R.p),
-                tei);
     k_gather_pairs<<<grid_of(n * (n + 1) / 2 * naux), 256, 0, s>>>(static_cast<const double*>(R.p), te, n, naux,
                                                                    static_cast<double*>(out.p));
     cudaMemcpyAsync(dEdI3, out.p, static_cast<size_t>(n * (n + 1) / 2) * naux * sizeof(double),
                     cudaMemcpyDeviceToHost, s);
   }
   if (dEdPQ) {
-    // G = 1/2 sum_e omega_e Gamma[Q][e] B[R][e] (omega = 2 off-diagonal tiles); dE/dV = -M^T G M
-    if ((rc = chk(ensure(ctx, Gm, static_cast<size_t>(naux) * naux * sizeof(double), "grad G"))) ||
-        (rc = chk(ensure(ctx, T1, static_cast<size_t>(naux) * naux * sizeof(double), "grad T1"))))
-      return rc;
-    k_scale_offdiag<<<grid_of(naux * te), 256, 0, s>>>(pGam, naux, ntile, 2.0, 1.0);
-    const double half = 0.5, mone = -1.0;
-    cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, na, na, tei, &half, pGam, tei, static_cast<const double*>(ctx->B.p), tei,
-                &zero, static_cast<double*>(Gm.p), na);
-    // T1 = G M_cm^T ; dEdPQ = -M_cm T1   (M_cm = M^T as a column-major naux x naux block, ld nauxp)
+    // dE/dV = -M^T G M:  T1 = G M_cm^T ; dEdPQ = -M_cm T1  (M_cm = M^T as a column-major naux x naux block, ld nauxp)
+    const double mone = -1.0;
     cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, na, na, na, &one, static_cast<const double*>(Gm.p), na, pM, nap, &zero,
                 static_cast<double*>(T1.p), na);
     cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, na, na, na, &mone, pM, nap, static_cast<const double*>(T1.p), na, &zero,
                 static_cast<double*>(Gm.p), na);
     cudaMemcpyAsync(dEdPQ, Gm.p, static_cast<size_t>(naux) * naux * sizeof(double), cudaMemcpyDeviceToHost, s);
   }
+  ctx->stats.grad_qchunk = qc;
   rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_grad");
   cleanup();
   (void)nt;

@@ -38,20 +38,28 @@ constexpr int kRedBlocks = 256;
 constexpr int kRedThreads = 256;
 constexpr int kOutSlots = 2 + 32 * 33 / 2;  // energy, error, lower triangle of a 32 x 32 Pulay matrix
 
-// partial[b] = sum over a grid-stride slice of f(i)
+// partial[b] (+ its compensation at partial[kRedBlocks + b]) = compensated sum over a grid-stride
+// slice of f(i); the energy, DIIS inner products and norms all go through it.
 template <typename F>
 __global__ void k_reduce_partial(F f, long n, double* __restrict__ partial) {
-  double acc = 0.0;
+  double s = 0.0, c = 0.0;
   for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<long>(gridDim.x) * blockDim.x)
-    acc += f(i);
-  __shared__ double sh[kRedThreads / 32];
-  acc = warp_sum(acc);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    neumaier_add(s, c, f(i));
+  __shared__ double sh[2][kRedThreads / 32];
+  warp_sum_comp(s, c);
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = s;
+    sh[1][threadIdx.x >> 5] = c;
+  }
   __syncthreads();
   if (threadIdx.x < 32) {
-    double v = threadIdx.x < kRedThreads / 32 ? sh[threadIdx.x] : 0.0;
-    v = warp_sum(v);
-    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    double v = threadIdx.x < kRedThreads / 32 ? sh[0][threadIdx.x] : 0.0;
+    double w = threadIdx.x < kRedThreads / 32 ? sh[1][threadIdx.x] : 0.0;
+    warp_sum_comp(v, w);
+    if (threadIdx.x == 0) {
+      partial[blockIdx.x] = v;
+      partial[kRedBlocks + blockIdx.x] = w;
+    }
   }
 }
 
@@ -73,17 +81,22 @@ __global__ void k_reduce_max_partial(F f, long n, double* __restrict__ partial) 
   }
 }
 
-// out[slot] = sum (or max) of the kRedBlocks partials, in a fixed order
+// out[slot] = sum (compensated, partials and their compensations) or max of the kRedBlocks
+// partials, in a fixed order.
 __global__ void k_reduce_final(const double* __restrict__ partial, int is_max, double* __restrict__ out, int slot) {
-  double v = (threadIdx.x < kRedBlocks) ? partial[threadIdx.x] : 0.0;
-  __shared__ double sh[kRedBlocks];
-  sh[threadIdx.x] = v;
-  __syncthreads();
-  for (int s = kRedBlocks / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) sh[threadIdx.x] = is_max ? fmax(sh[threadIdx.x], sh[threadIdx.x + s]) : sh[threadIdx.x] + sh[threadIdx.x + s];
-    __syncthreads();
+  if (threadIdx.x != 0) return;
+  if (is_max) {
+    double m = 0.0;
+    for (int b = 0; b < kRedBlocks; ++b) m = fmax(m, partial[b]);
+    out[slot] = m;
+  } else {
+    double s = 0.0, c = 0.0;
+    for (int b = 0; b < kRedBlocks; ++b) {
+      neumaier_add(s, c, partial[b]);
+      c += partial[kRedBlocks + b];
+    }
+    out[slot] = s + c;
   }
-  if (threadIdx.x == 0) out[slot] = sh[0];
 }
 
 struct DotF {
@@ -313,7 +326,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       (rc = ensure(ctx, dT1, b_nn, "scf T1")) || (rc = ensure(ctx, dT2, b_nn, "scf T2")) ||
       (rc = ensure(ctx, dE, b_nn, "scf E")) || (rc = ensure(ctx, dU, b_nn, "scf U")) ||
       (rc = ensure(ctx, dW, n * sizeof(double), "scf w")) || (rc = ensure(ctx, info, sizeof(int), "scf info")) ||
-      (rc = ensure(ctx, red, kRedBlocks * sizeof(double), "scf reduce")) ||
+      (rc = ensure(ctx, red, 2 * kRedBlocks * sizeof(double), "scf reduce")) ||
       (rc = ensure(ctx, out, kOutSlots * sizeof(double), "scf out")) ||
       (rc = ensure(ctx, ring_F, static_cast<size_t>(m_max) * b_nn, "scf DIIS F")) ||
       (rc = ensure(ctx, ring_E, static_cast<size_t>(m_max) * b_nn, "scf DIIS e"))) {

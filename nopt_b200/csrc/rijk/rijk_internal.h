@@ -59,6 +59,7 @@ struct rijk_ctx {
   long q0 = 0, nq = 0;  // aux functions [q0, q0 + nq) held in B (all of them unless rijk_set_aux_range)
   int metric_form = RIJK_METRIC_INVSQRT;
   bool have_metric = false, have_b = false;
+  long grad_qchunk = 0;  // aux functions per chunk of rijk_grad (0: as many as HBM holds)
 
   rijk::DeviceBuf M;      // metric factor, naux x naux
   rijk::DeviceBuf B;      // fitted tensor, naux x ntile x TILE2 doubles

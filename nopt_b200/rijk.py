@@ -40,7 +40,8 @@ class Stats(ctypes.Structure):
                 ("bytes_b_mixed", ctypes.c_long), ("kernels_last_fock", ctypes.c_int),
                 ("profiled_stages", ctypes.c_int), ("ms_stage", ctypes.c_double * 12),
                 ("stage_names", (ctypes.c_char * 24) * 12), ("ms_setup_ints", ctypes.c_double),
-                ("kernels_setup_ints", ctypes.c_int), ("q0", ctypes.c_long), ("nq", ctypes.c_long)]
+                ("kernels_setup_ints", ctypes.c_int), ("q0", ctypes.c_long), ("nq", ctypes.c_long),
+                ("grad_qchunk", ctypes.c_long)]
 
 
 class BasisT(ctypes.Structure):
@@ -110,6 +111,7 @@ def lib():
         L.rijk_mo_calc.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long, _dp, _dp, _dp, _dp, _dp]
         L.rijk_mo_ints_aaag.argtypes = [_vp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
         L.rijk_soscf_hess_ints.argtypes = [_vp, _dp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
+        L.rijk_set_grad_chunk.argtypes = [_vp, ctypes.c_long]
         L.rijk_save.argtypes = [_vp, ctypes.c_char_p]
         L.rijk_load.argtypes = [_vp, ctypes.c_char_p]
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
@@ -309,6 +311,10 @@ class FockBuilder:
         self._check(lib().rijk_mo_ints(self._h, _p(D), _p(J), _p(K), _p(out), _p(M0), _p(_c(MO_VEC1)),
                                        _p(_c(MO_VEC2)), int(n_c), int(n_a), int(t)))
         return out, J, K
+
+    def set_grad_chunk(self, q_per_chunk):
+        """Aux functions per chunk of grad's Gamma stage (0: automatic, from free HBM)."""
+        self._check(lib().rijk_set_grad_chunk(self._h, int(q_per_chunk)))
 
     def grad(self, MO, n_c, H, e_nuc, want_3c=False, want_metric=False):
         """(E, dE/dMO (n_c x n), dE/d(P|mu nu) packed [pair][P] or None, dE/d(P|Q) or None)."""

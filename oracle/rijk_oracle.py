@@ -227,21 +227,24 @@ def adjoint_reference(I3_packed, M, H, MO, n_c, Enuc):
     il = np.tril_indices(n)
     Bf[:, il[0], il[1]] = Bp
     Bf[:, il[1], il[0]] = Bp
+    Bm = Bf.reshape(naux, n * n)
     C = MO[:n_c]
     D = C.T @ C
-    w = np.einsum("qmn,mn->q", Bf, D)
-    X = np.einsum("im,qmn->qin", C, Bf)
-    Y = np.einsum("qin,jn->qij", X, C)
-    J = np.einsum("q,qmn->mn", w, Bf)
-    K = np.einsum("qim,qin->mn", X, X)
+    w = Bm @ D.reshape(-1)                                   # <B^Q, D>
+    X = np.matmul(C[None], Bf)                               # X^Q = C B^Q        (naux, n_c, n)
+    Y = np.matmul(X, C.T[None])                              # Y^Q = C B^Q C^T    (naux, n_c, n_c)
+    J = (w @ Bm).reshape(n, n)
+    Xm = X.reshape(naux * n_c, n)
+    K = Xm.T @ Xm                                            # sum_Q X^Q^T X^Q
     F = H + 2 * J - K
     E = 2 * np.sum(H * D) + 2 * np.sum(w * w) - np.sum(Y * Y) + Enuc
     dC = 4 * C @ F
-    Gam = 4 * w[:, None, None] * D[None] - 2 * np.einsum("im,qij,jn->qmn", C, Y, C)
-    d3f = np.einsum("qp,qmn->pmn", M, Gam)
+    Gam = 4 * w[:, None, None] * D[None] - 2 * np.matmul(np.matmul(C.T[None], Y), C[None])
+    Gm = Gam.reshape(naux, n * n)
+    d3f = (M.T @ Gm).reshape(naux, n, n)                     # sum_Q M_QP Gamma^Q
     fac = np.where(il[0] == il[1], 1.0, 2.0)
     d3 = (d3f[:, il[0], il[1]] * fac).T.copy()
-    G = 0.5 * np.einsum("qmn,rmn->qr", Gam, Bf)
+    G = 0.5 * Gm @ Bm.T
     dV = -M.T @ G @ M
     return E, dC, d3, dV
 
