@@ -64,9 +64,35 @@ def parse():
     return ap.parse_args()
 
 
+class SyntheticSystem:
+    """Seeded random inputs of a chosen size (workload "rand:n=..,naux=..,nocc=.."): packed
+    three-centre entries ~ N(0,1) e^{-|mu-nu|/n}, a well-conditioned metric, a random symmetric H and
+    S = 1.  For kernel timing and profiling at sizes the molecules do not give; no SCF."""
+
+    def __init__(self, spec, seed):
+        kv = dict(x.split("=") for x in spec.split(","))
+        self.n, self.naux, self.nocc = int(kv["n"]), int(kv["naux"]), int(kv["nocc"])
+        rng = np.random.default_rng(seed)
+        n, na = self.n, self.naux
+        A = rng.normal(size=(na, na))
+        self.V = A @ A.T / na + np.eye(na)
+        mu, nu = np.tril_indices(n)
+        self.I3 = rng.normal(size=(mu.size, na)) * np.exp(-np.abs(mu - nu) / n)[:, None]
+        Hm = rng.normal(size=(n, n))
+        self.H = (Hm + Hm.T) / np.sqrt(n)
+        self.S = np.eye(n)
+        self.Enuc = 0.0
+        self.orb = self.aux = None
+        self.synthetic = True
+
+
 def build_system(workload, seed, ri_integrals=True):
     from nopt_b200 import ints
     from nopt_b200.molecules import WORKLOADS
+    if workload.startswith("rand:"):
+        t = time.time()
+        si = SyntheticSystem(workload[5:], seed)
+        return si, time.time() - t, (None, None)
     fac, ob, ab = WORKLOADS[workload]
     mol = fac(seed)
     t = time.time()
@@ -208,6 +234,9 @@ def main():
     from nopt_b200 import rijk
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    synthetic = args.workload.startswith("rand:")
+    if synthetic:  # no basis: integrals come from the seeded generator, set up through rijk_set_3c
+        args.setup, args.no_scf = "host", True
     # host RI integrals only where something needs them: the host set-up path or the CPU baseline
     need_host_ri = args.setup == "host" or (not args.no_cpu and rank == 0 and world == 1)
     si, tint, (ob, ab) = build_system(args.workload, args.seed, ri_integrals=need_host_ri)
@@ -418,7 +447,7 @@ def main():
 
     # per-iteration errors of the mixed form along an FP64 SCF path: at each iteration's density both
     # forms are built; max |dJ|, max |dK| and the energy difference tr((2 dJ - dK) D) are recorded
-    if isinstance(mixed, dict) and "unavailable" not in mixed and not sharded:
+    if isinstance(mixed, dict) and "unavailable" not in mixed and not sharded and not synthetic:
         s_, U_ = np.linalg.eigh(si.S)
         Xo = U_[:, s_ > 1e-10] / np.sqrt(s_[s_ > 1e-10])
         D0, R0 = si.sad()
@@ -489,7 +518,9 @@ def main():
                "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
                "scaling": "strong" if sharded else "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": WORKLOAD_NAMES.get(args.workload, args.workload),
+               "config": {"workload": WORKLOAD_NAMES.get(args.workload, args.workload if not synthetic else
+                                                        "synthetic " + args.workload[5:].replace(",", " ") +
+                                                        " (random packed B ~ N(0,1) e^-|mu-nu|/n)"),
                           "n": n, "naux": naux, "nocc": nocc,
                           "parallelism": ("aux-sharded x%d" % world) if sharded else
                                          ("replicas x%d" % world if world > 1 else "single"),
