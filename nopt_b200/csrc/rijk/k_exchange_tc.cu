@@ -320,14 +320,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 }
 
 // ------------------------------------------------------------------ K4: SYRK ----
+// K = X^T X over split-K ranges of kdim.  The contraction of one CTA runs in segments of `seg`
+// 64-wide chunks (12 MMAs each: 4 k-steps x 3 split terms), alternating between two TMEM
+// accumulators; the epilogue warps fold each finished segment into fp32 registers
+// (accumulate_segment) while the next one is computed.  A TMEM accumulator thus never sums more
+// than one segment, which keeps the tensor core's own fp32 accumulation error at the scale of a
+// segment's partial sum instead of the whole range's.
 struct SyrkParams {
   long kdim, kper;
-  int npad2, ntile64, stages;
-  float* Kpart;  // fp32 partials: the TMEM accumulators stored as they are
+  int npad2, ntile64, stages, seg;
+  float* Kpart;  // fp32 partials, one 64 x 64 tile set per split
   int* err;
 };
 
 constexpr uint32_t kSyOpBytes = 128 * 128;  // 128 rows x 64 bf16
+#ifndef RIJK_SYRK_SEG
+#define RIJK_SYRK_SEG 4
+#endif
+constexpr int kSySeg = RIJK_SYRK_SEG;  // 64-wide chunks per TMEM accumulation segment
 constexpr uint32_t kSyStage = 4 * kSyOpBytes;
 
 __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant__ CUtensorMap mapX, SyrkParams p) {
@@ -336,8 +346,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * kSyStage);
   uint64_t* empty = full + S;
-  uint64_t* tfull = empty + S;
-  uint64_t* drain = tfull + 1;
+  uint64_t* tfull = empty + S;   // [2] accumulator b holds a finished segment
+  uint64_t* tempty = tfull + 2;  // [2] accumulator b has been folded into registers
+  uint64_t* drain = tempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -348,6 +359,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
   const long k0 = s * p.kper;
   const long k1 = std::min(k0 + p.kper, p.kdim);
   const int nch = static_cast<int>((k1 - k0 + 63) / 64);
+  const int seg = p.seg;
+  const int nseg = (nch + seg - 1) / seg;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
@@ -355,13 +368,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
-    mbar_init(tfull, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tfull[i], 1);
+      mbar_init(&tempty[i], 4);  // the four epilogue warps
+    }
     mbar_init(drain, 1);
     *abort = 0;
     fence_barrier_init();
   }
   if (warp == 1) {
-    tmem_alloc(tmem_slot, 128);
+    tmem_alloc(tmem_slot, 256);
     tmem_relinquish();
   }
   tc_fence_before();
@@ -412,12 +428,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
+      int g = 0, kq = 0;  // segment of chunk c and its position in the segment
       for (int c = 0; c < nch; ++c) {
+        const int buf = g & 1;
+        if (kq == 0) {  // accumulator buf was last used by segment g - 2
+          if (!mbar_wait(&tempty[buf], ((g >> 1) & 1) ^ 1, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+        }
         if (!mbar_wait(&full[stage], phase, abort)) {
           ok = false;
           break;
         }
         tc_fence_after();
+        const uint32_t acc = tmem + buf * 128;
         const uint32_t sa = smem_u32(smem + stage * kSyStage);
         const uint32_t ah = sa, al = sa + kSyOpBytes;
         const uint32_t bh = diag ? ah : sa + 2 * kSyOpBytes, bl = diag ? al : sa + 3 * kSyOpBytes;
@@ -425,11 +451,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
         for (int kk = 0; kk < 4; ++kk) {
           const uint64_t dah = sw128_desc(ah + kk * 32, kKdesc), dal = sw128_desc(al + kk * 32, kKdesc);
           const uint64_t dbh = sw128_desc(bh + kk * 32, kKdesc), dbl = sw128_desc(bl + kk * 32, kKdesc);
-          umma_bf16(tmem, dah, dbh, id, (c | kk) != 0 ? 1u : 0u);
-          umma_bf16(tmem, dah, dbl, id, 1u);
-          umma_bf16(tmem, dal, dbh, id, 1u);
+          umma_bf16(acc, dah, dbh, id, (kq | kk) != 0 ? 1u : 0u);
+          umma_bf16(acc, dah, dbl, id, 1u);
+          umma_bf16(acc, dal, dbh, id, 1u);
         }
         umma_commit(&empty[stage]);
+        if (kq == seg - 1 || c == nch - 1) umma_commit(&tfull[buf]);
+        if (++kq == seg) {
+          kq = 0;
+          ++g;
+        }
         if (++stage == S) {
           stage = 0;
           phase ^= 1;
@@ -439,29 +470,57 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
         *abort = 1;
         atomicOr(p.err, DEVERR_TIMEOUT);
       }
-      umma_commit(tfull);
       umma_commit(drain);
       volatile int never = 0;
       if (!mbar_wait(drain, 0, &never)) atomicOr(p.err, DEVERR_TIMEOUT);
     }
   } else {
     const int q = warp & 3;
-    if (mbar_wait(tfull, 0, abort) && !*abort) {
+    const int row = q * 32 + lane;
+    const long ra = 2 * a + row / 64;  // the same for the 32 lanes of a warp
+    const int r = row % 64;
+    float acc[128];
+#pragma unroll
+    for (int j = 0; j < 128; ++j) acc[j] = 0.f;
+    bool ok = nseg > 0;
+    for (int g = 0; g < nseg; ++g) {
+      const int buf = g & 1;
+      // warp-uniform outcome: the TMEM loads below are .sync.aligned
+      if (!__all_sync(0xffffffffu, mbar_wait(&tfull[buf], (g >> 1) & 1, abort))) {
+        ok = false;
+        break;
+      }
       tc_fence_after();
-      const int row = q * 32 + lane;
-      const long ra = 2 * a + row / 64;
-      const int r = row % 64;
-#pragma unroll 1
+      const uint32_t t = tmem + buf * 128 + (static_cast<uint32_t>(q * 32) << 16);
+      if (g + 1 < nseg) {
+        accumulate_segment<32>(t, acc);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+        continue;
+      }
+      if (__any_sync(0xffffffffu, *abort)) {
+        ok = false;
+        break;
+      }
+      // last segment: fold and store 16 columns at a time, so the stores interleave with the loads
+#pragma unroll
       for (int c0 = 0; c0 < 128; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c0, v);
+        uint32_t v[16];
+        tmem_ld16_nowait(t + c0, v);
+        tmem_wait_ld();
         const long cb = 2 * b + c0 / 64;
         if (diag && ra < cb) continue;  // upper-right sub-tile of a diagonal tile: its mirror is stored
         float* out = p.Kpart + (s * p.ntile64 + tri_index(ra, cb)) * TILE2 + r * TILE + (c0 % 64);
 #pragma unroll
-        for (int j = 0; j < 16; j += 4) *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4*>(out + j) =
+              make_float4(acc[c0 + j] + __uint_as_float(v[j]), acc[c0 + j + 1] + __uint_as_float(v[j + 1]),
+                          acc[c0 + j + 2] + __uint_as_float(v[j + 2]), acc[c0 + j + 3] + __uint_as_float(v[j + 3]));
       }
-    } else if (lane == 0) {
+    }
+    if (!ok && lane == 0) {
+      *abort = 1;
       atomicOr(p.err, DEVERR_TIMEOUT);
     }
   }
@@ -469,7 +528,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, 128);
+    tmem_dealloc(tmem, 256);
   }
 }
 
@@ -480,23 +539,32 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc(const __grid_constant
 // (rank 0) issues M = 256, N = 256 MMAs over both CTAs' shared memory.  Each operand byte
 // crosses L2 -> SM once for twice the FLOPs of a 128 x 128 tile.  Both CTAs' TMA loads complete
 // on the leader's stage barrier, which alone expects the pair's bytes; the leader's commits
-// release the stage (and signal the accumulator) in both CTAs.  A last 256-row panel that
-// runs past npad2 computes rows and columns that are never stored.
+// release the stage (and signal a finished accumulator) in both CTAs.  As in k_syrk_tc the
+// contraction runs in segments over two TMEM accumulators (2 x 256 columns); eight epilogue
+// warps per CTA fold them into registers (warp w reads TMEM lanes 32 (w % 4) .., columns
+// 128 h .. 128 h + 127 with h = (w - 2) / 4) and report each fold to the leader's barrier.
+// (Ten warps: the register file is split over four sub-partitions, so a thread may hold 168
+// registers; more warps would leave too few for the 128 accumulators.)  A
+// last 256-row panel that runs past npad2 computes rows and columns that are never stored.
+constexpr int kPairThreads = 320;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+
 struct SyrkPairParams {
   long kdim, kper;
-  int npad2, nt2, ntile64, stages;
+  int npad2, nt2, ntile64, stages, seg;
   float* Kpart;
   int* err;
 };
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constant__ CUtensorMap mapX, SyrkPairParams p) {
+__global__ void __launch_bounds__(kPairThreads, 1)
+    k_syrk_tc2(const __grid_constant__ CUtensorMap mapX, SyrkPairParams p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
   const int S = p.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * kSyStage);
   uint64_t* empty = full + S;
-  uint64_t* tfull = empty + S;
-  uint64_t* drain = tfull + 1;
+  uint64_t* tfull = empty + S;   // [2]
+  uint64_t* tempty = tfull + 2;  // [2] on the leader: 16 arrivals, 8 epilogue warps of each CTA
+  uint64_t* drain = tempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -509,6 +577,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constan
   const long k0 = s * p.kper;
   const long k1 = std::min(k0 + p.kper, p.kdim);
   const int nch = static_cast<int>((k1 - k0 + 63) / 64);
+  const int seg = p.seg;
+  const int nseg = (nch + seg - 1) / seg;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
@@ -516,13 +586,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constan
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
-    mbar_init(tfull, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tfull[i], 1);
+      mbar_init(&tempty[i], 16);
+    }
     mbar_init(drain, 1);
     *abort = 0;
     fence_barrier_init();
   }
   if (warp == 1) {
-    tmem_alloc_pair(tmem_slot, 256);
+    tmem_alloc_pair(tmem_slot, 512);
     tmem_relinquish_pair();
   }
   tc_fence_before();
@@ -577,12 +650,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constan
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
+      int g = 0, kq = 0;  // segment of chunk c and its position in the segment
       for (int c = 0; c < nch; ++c) {
+        const int buf = g & 1;
+        if (kq == 0) {  // both CTAs have folded accumulator buf (segment g - 2)
+          if (!mbar_wait(&tempty[buf], ((g >> 1) & 1) ^ 1, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+        }
         if (!mbar_wait(&full[stage], phase, abort)) {
           ok = false;
           break;
         }
         tc_fence_after();
+        const uint32_t acc = tmem + buf * 256;
         const uint32_t sa = smem_u32(smem + stage * kSyStage);
         const uint32_t ah = sa, al = sa + kSyOpBytes;
         const uint32_t bh = diag ? ah : sa + 2 * kSyOpBytes, bl = diag ? al : sa + 3 * kSyOpBytes;
@@ -590,11 +673,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constan
         for (int kk = 0; kk < 4; ++kk) {
           const uint64_t dah = sw128_desc(ah + kk * 32, kKdesc), dal = sw128_desc(al + kk * 32, kKdesc);
           const uint64_t dbh = sw128_desc(bh + kk * 32, kKdesc), dbl = sw128_desc(bl + kk * 32, kKdesc);
-          umma_bf16_pair(tmem, dah, dbh, id, (c | kk) != 0 ? 1u : 0u);
-          umma_bf16_pair(tmem, dah, dbl, id, 1u);
-          umma_bf16_pair(tmem, dal, dbh, id, 1u);
+          umma_bf16_pair(acc, dah, dbh, id, (kq | kk) != 0 ? 1u : 0u);
+          umma_bf16_pair(acc, dah, dbl, id, 1u);
+          umma_bf16_pair(acc, dal, dbh, id, 1u);
         }
         umma_commit_pair(&empty[stage], 0x3);
+        if (kq == seg - 1 || c == nch - 1) umma_commit_pair(&tfull[buf], 0x3);
+        if (++kq == seg) {
+          kq = 0;
+          ++g;
+        }
         if (++stage == S) {
           stage = 0;
           phase ^= 1;
@@ -604,27 +692,54 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constan
         *abort = 1;
         atomicOr(p.err, DEVERR_TIMEOUT);
       }
-      umma_commit_pair(tfull, 0x3);
       umma_commit_pair(drain, 0x3);
     }
   } else {
-    const int q = warp & 3;
-    if (mbar_wait(tfull, 0, abort) && !*abort) {
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    const long row = a * 256 + rank * 128 + q * 32 + lane;  // row of K
+    const long ra = row / 64;  // the same for the 32 lanes of a warp
+    const int r = static_cast<int>(row % 64);
+    float acc[128];
+#pragma unroll
+    for (int j = 0; j < 128; ++j) acc[j] = 0.f;
+    bool ok = nseg > 0;
+    for (int g = 0; g < nseg; ++g) {
+      const int buf = g & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(&tfull[buf], (g >> 1) & 1, abort))) {
+        ok = false;
+        break;
+      }
       tc_fence_after();
-      const long row = a * 256 + rank * 128 + q * 32 + lane;  // row of K
-      const long ra = row / 64;
-      const int r = static_cast<int>(row % 64);
-#pragma unroll 1
-      for (int c0 = 0; c0 < 256; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c0, v);
-        const long cb = (b * 256 + c0) / 64;
+      const uint32_t t = tmem + buf * 256 + h * 128 + (static_cast<uint32_t>(q * 32) << 16);
+      if (g + 1 < nseg) {
+        accumulate_segment<16>(t, acc);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(&tempty[buf], 0);
+        continue;
+      }
+      if (__any_sync(0xffffffffu, *abort)) {
+        ok = false;
+        break;
+      }
+      // last segment: fold and store 16 columns at a time, so the stores interleave with the loads
+#pragma unroll
+      for (int c0 = 0; c0 < 128; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16_nowait(t + c0, v);
+        tmem_wait_ld();
+        const long cb = (b * 256 + h * 128 + c0) / 64;
         if (ra < cb || ra >= p.nt2 || cb >= p.nt2) continue;  // upper triangle, or past npad2
         float* out = p.Kpart + (s * p.ntile64 + tri_index(ra, cb)) * TILE2 + r * TILE + (c0 % 64);
 #pragma unroll
-        for (int j = 0; j < 16; j += 4) *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4*>(out + j) =
+              make_float4(acc[c0 + j] + __uint_as_float(v[j]), acc[c0 + j + 1] + __uint_as_float(v[j + 1]),
+                          acc[c0 + j + 2] + __uint_as_float(v[j + 2]), acc[c0 + j + 3] + __uint_as_float(v[j + 3]));
       }
-    } else if (lane == 0) {
+    }
+    if (!ok && lane == 0) {
+      *abort = 1;
       atomicOr(p.err, DEVERR_TIMEOUT);
     }
   }
@@ -638,7 +753,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_syrk_tc2(const __grid_constan
   cluster_sync_all();  // neither CTA frees its TMEM or exits while the pair's work may touch it
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc_pair(tmem, 256);
+    tmem_dealloc_pair(tmem, 512);
   }
 }
 
@@ -824,6 +939,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
     pp.ntile64 = static_cast<int>(ntile2);
     pp.Kpart = Kpart32;
     pp.err = static_cast<int*>(ctx->err.p);
+    pp.seg = kSySeg;
     pp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
     const size_t smem2 = static_cast<size_t>(pp.stages) * kSyStage + 1024 + 256;
     static bool attr2 = false;
@@ -833,7 +949,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
     }
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(static_cast<unsigned>(2 * tiles256), static_cast<unsigned>(nsplit2));
-    cfg.blockDim = dim3(kTcThreads);
+    cfg.blockDim = dim3(kPairThreads);
     cfg.dynamicSmemBytes = smem2;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -860,6 +976,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   sp.ntile64 = static_cast<int>(ntile2);
   sp.Kpart = Kpart32;
   sp.err = static_cast<int*>(ctx->err.p);
+  sp.seg = kSySeg;
   sp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
   size_t smem = static_cast<size_t>(sp.stages) * kSyStage + 1024 + 256;
   static bool attr = false;

@@ -1,6 +1,7 @@
 // tc_util.cuh — Blackwell (sm_100a) primitives used by the mixed-precision exchange kernels:
 // mbarriers with bounded waits, TMA 2-D tile loads (no multicast), tcgen05 TMEM allocation,
-// UMMA (tcgen05.mma kind::f16) issue/commit and TMEM -> register loads.
+// UMMA (tcgen05.mma kind::f16) issue/commit, TMEM -> register loads, and the register-side
+// accumulation of short TMEM segments (accumulate_segment).
 //
 // Shared-memory operand descriptors (64-bit) follow the sm_100 UMMA format:
 //   bits  0-13  start address >> 4        bits 16-29  leading-dimension byte offset >> 4
@@ -112,6 +113,41 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// The same load without its wait; tmem_wait_ld() completes every load issued before it.
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// acc[j] += column j of this thread's TMEM lane at taddr, j < NCOL: a segment of a long
+// contraction accumulated in TMEM is folded into fp32 registers with round-to-nearest adds, so
+// no single TMEM accumulator runs over more than one short segment.  WIDE columns (16 or 32)
+// are loaded per wait; 16 suits kernels with a tighter register budget.
+template <int WIDE, int NCOL>
+__device__ __forceinline__ void accumulate_segment(uint32_t taddr, float (&acc)[NCOL]) {
+  static_assert((WIDE == 16 || WIDE == 32) && NCOL % WIDE == 0, "whole groups of 16 or 32 columns");
+#pragma unroll
+  for (int c0 = 0; c0 < NCOL; c0 += WIDE) {
+    uint32_t r[2][16];
+    tmem_ld16_nowait(taddr + c0, r[0]);
+    if (WIDE == 32) tmem_ld16_nowait(taddr + c0 + 16, r[1]);
+    tmem_wait_ld();
+#pragma unroll
+    for (int j = 0; j < WIDE; ++j) acc[c0 + j] += __uint_as_float(r[j / 16][j % 16]);
+  }
+}
+
+// Arrive once on the barrier at `bar`'s offset in the shared memory of cluster CTA `rank`.
+__device__ __forceinline__ void mbar_arrive_cluster(uint64_t* bar, uint32_t rank) {
+  uint32_t remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(remote) : "r"(smem_u32(bar)), "r"(rank));
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(remote) : "memory");
 }
 
 __host__ __device__ constexpr uint64_t sw128_desc_bits(uint32_t lbo_bytes, uint32_t sbo_bytes) {

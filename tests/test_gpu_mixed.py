@@ -72,3 +72,29 @@ def test_mixed_k_ragged_random(n, naux, nocc):
     I3 = rng.normal(size=(n * (n + 1) // 2, naux)) * 0.1
     DM, MO = _state(n, nocc, 3)
     _check(V, I3, n, nocc, DM, MO)
+
+
+def test_mixed_k_long_contraction_c40h82():
+    """C40H82 cc-pVDZ/JKFIT (n = 970, naux = 4686, n_c = 161) at the first SCF density from the SAD
+    start.  The CTA-pair SYRK contracts a few hundred 64-wide chunks per split; folding TMEM segments
+    of four chunks into fp32 registers keeps tr(D dK) of one build near 1e-3 Eh (a single TMEM
+    accumulation over each split gave 1.2e-2 Eh, 12x more)."""
+    from nopt_b200.molecules import WORKLOADS
+    fac, ob, ab = WORKLOADS["c40h82_dz"]
+    si = ints.SystemIntegrals(fac(0), ob, ab, ri_integrals=False)
+    n, nocc = si.n, si.nocc
+    s_, U_ = np.linalg.eigh(si.S)
+    Xo = U_[:, s_ > 1e-10] / np.sqrt(s_[s_ > 1e-10])
+    with rijk.FockBuilder(0) as fb:
+        fb.set_basis(si.orb, si.aux, rijk.METRIC_INVSQRT)
+        D0, R0 = si.sad()
+        Jg, Kg = fb.dm_to_f_transform_ri(D0, R0, R0.shape[0])
+        _, Cp = np.linalg.eigh(Xo.T @ (si.H + 2 * Jg - Kg) @ Xo)
+        MO = (Xo @ Cp).T[:nocc].copy()
+        DM = MO.T @ MO
+        J64, K64 = fb.dm_to_f_transform_ri(DM, MO, nocc, rijk.PREC_FP64)
+        Jm, Km = fb.dm_to_f_transform_ri(DM, MO, nocc, rijk.PREC_MIXED)
+    dK = Km - K64
+    assert float(np.max(np.abs(dK))) < 1.5e-4
+    assert abs(float(np.sum(DM * dK))) < 3e-3
+    assert float(np.max(np.abs(Jm - J64))) < 1e-4
