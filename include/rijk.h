@@ -191,7 +191,10 @@ typedef struct {
   int converger;          /* RIJK_CONV_DIIS (default) or RIJK_CONV_SOSCF, the reference's RHF step:
                              L-BFGS on the occupied-virtual rotations with the diagonal Hessian
                              4 (e_a - e_i), rotation I + X - X^T orthonormalised by Gram-Schmidt
-                             (src/SCF.cpp:125-174, src/converger_2_1.cpp:55-125, src/l-bfgs_2_1.cpp) */
+                             (src/SCF.cpp:125-174, src/converger_2_1.cpp:55-125, src/l-bfgs_2_1.cpp);
+                             or RIJK_CONV_DIIS_SOSCF: DIIS while the builds are mixed, the SOSCF
+                             step (and its convergence test) from the switch to FP64 on, entered
+                             as the reference enters it: one plain diagonalisation first         */
   double conv_grad;       /* SOSCF: converged when max |4 F_ai| < conv_grad; default 1e-7          */
   double conv_energy;     /* SOSCF: or when |E - E_previous| < conv_energy; default 1e-10          */
   int lbfgs_vectors;      /* SOSCF: curvature pairs kept, 1 .. 32; default min(n_mo, 20, max_iter)  */
@@ -199,12 +202,15 @@ typedef struct {
 
 #define RIJK_CONV_DIIS 0
 #define RIJK_CONV_SOSCF 1
+#define RIJK_CONV_DIIS_SOSCF 2
 
 typedef struct {
-  double energy;          /* E = tr(F D) + tr(H D) + e_nuc of the converged FP64 Fock build     */
+  double energy;          /* E = tr(F D) + tr(H D) + e_nuc of the last FP64 Fock build, as the
+                             reference reports it (src/SCF.cpp:134-156); a run that ends in the
+                             mixed phase gets one more FP64 build for it                        */
   double dm_rms;          /* last RMS density change                                          */
-  double diis_err;        /* last max |X^T (F D S - S D F) X|; with SOSCF, the last max |4 F_ai| */
-  int iterations;         /* Fock builds, the final FP64 one included                          */
+  double diis_err;        /* last max |X^T (F D S - S D F) X|; in SOSCF steps, max |4 F_ai|     */
+  int iterations;         /* Fock builds                                                       */
   int iterations_mixed;   /* of which in the mixed form                                        */
   int converged;
   int nmo;                /* orbitals kept after removing linear dependence                    */
@@ -215,14 +221,16 @@ typedef struct {
   double ms_diag_phase;   /* wall time of diagonalisation + new density                        */
   int history_len;        /* entries of the per-iteration trace below (first 128 iterations)   */
   double history_energy[128];
-  double history_diis_err[128];  /* per build: the DIIS error, or max |4 F_ai| with SOSCF          */
+  double history_diis_err[128];  /* per build: the DIIS error, or max |4 F_ai| in SOSCF steps      */
   int history_mixed[128]; /* 1 where the iteration used the mixed form                          */
 } rijk_scf_result_t;
 
 /* Restricted Hartree-Fock on the GPU around the Fock build: the reference's RHF loop
  * (src/SCF.cpp:78-223).  The converger is Pulay DIIS on F D S - S D F (default) or, with
  * opts->converger = RIJK_CONV_SOSCF, the reference's own SOSCF/L-BFGS orbital-rotation step and
- * convergence test (max |4 F_ai| or |dE|); both reach the same energy.  H and S are n x n host
+ * convergence test (max |4 F_ai| or |dE|), or DIIS then SOSCF (RIJK_CONV_DIIS_SOSCF); all reach
+ * the same energy.  MO holds the eigenvectors of the last FP64 Fock matrix (the reference's
+ * closing diagonalisation, src/SCF.cpp:178).  H and S are n x n host
  * arrays; n_c occupied orbitals; the core-Hamiltonian guess (or opts' guess) starts it.
  * Diagonalisation, the converger's algebra and the energy are FP64 on the device.  MO (optional, n x n host) receives the orbitals, one per row, as the
  * reference's MO_VEC; E as in src/SCF.cpp:134. */

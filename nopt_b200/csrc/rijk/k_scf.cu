@@ -290,11 +290,12 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   if (o.lindep <= 0) o.lindep = 1e-10;
   if (o.conv_grad <= 0) o.conv_grad = 1e-7;      // RHF_GR_CON_DEFAULT (include/defaults.h:7)
   if (o.conv_energy <= 0) o.conv_energy = 1e-10;  // RHF_EN_CON_DEFAULT (include/defaults.h:6)
-  if (o.converger != RIJK_CONV_DIIS && o.converger != RIJK_CONV_SOSCF)
+  if (o.converger != RIJK_CONV_DIIS && o.converger != RIJK_CONV_SOSCF && o.converger != RIJK_CONV_DIIS_SOSCF)
     return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: unknown converger %d", o.converger);
   if (o.lbfgs_vectors < 0 || o.lbfgs_vectors > 32)
     return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: lbfgs_vectors outside 0 .. 32");
-  const bool soscf = o.converger == RIJK_CONV_SOSCF;
+  const bool soscf = o.converger == RIJK_CONV_SOSCF;         // SOSCF from the start
+  const bool hybrid = o.converger == RIJK_CONV_DIIS_SOSCF;   // DIIS, then SOSCF from the switch on
   int rc = check_fock_args(ctx, nocc, o.precision);
   if (rc) return rc;
   if (o.diis_size > 32) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: diis_size above 32");
@@ -461,9 +462,9 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       cleanup();
       return rc;
     }
-    if (diag(pF, soscf) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the guess Fock matrix failed");
+    if (diag(pF, soscf || hybrid) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the guess Fock matrix failed");
   } else {
-    if (diag(pH, soscf) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
+    if (diag(pH, soscf || hybrid) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
   }
   density(pD);
 
@@ -475,18 +476,143 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   result->history_len = 0;
   bool converged = false;
   std::vector<double> hout(8);
+  int last_prec = -1;  // precision of the last build (pF, pJ, pK hold its result)
   auto build = [&](int p) -> int {
     int r = fock_device_impl(ctx, pD, pC, nocc, pJ, pK, p);
     if (r) return r;
     k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
     ++nbuild;
     if (p == RIJK_PREC_MIXED) ++nmix;
+    last_prec = p;
     return RIJK_OK;
   };
+  int it_used = 0;              // iterations taken by the DIIS phase of the hybrid converger
+  bool run_soscf = soscf;       // the SOSCF loop runs (from the start, or after the DIIS phase)
+  bool soscf_from_diis = false; // it starts from DIIS orbitals (all of them, eigenvectors of pFex)
   double t_build = 0.0, t_diis = 0.0, t_diag = 0.0;
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto msec = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
-  if (soscf) {
+  if (!soscf) {
+    bool have_fex = false;  // pFex holds the matrix whose eigenvectors gave pD
+    for (int it = 0; it < o.max_iter; ++it) {
+      auto ta = now();
+      if ((rc = build(prec))) {
+        cleanup();
+        return rc;
+      }
+      // energy and DIIS error X^T (F D S - S D F) X
+      reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pF, ni, pD, ni, &zero, pT1, ni);   // F D
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pT1, ni, pS, ni, &zero, pT2, ni);  // F D S
+      k_antisym<<<grid_of(nn), 256, 0, s>>>(pT2, n, pT1);                                            // FDS - SDF
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, pT1, ni, pX, ni, &zero, pT2, ni);  // e X
+      double* slotE = rE + static_cast<size_t>(head) * nn;
+      double* slotF = rF + static_cast<size_t>(head) * nn;
+      cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT2, ni, &zero, slotE, nmi);  // X^T e X
+      cudaMemcpyAsync(slotF, pF, b_nn, cudaMemcpyDeviceToDevice, s);
+      reduce(AbsF{slotE}, nm * nm, 1, 1);
+      cudaEventRecord(ctx->ev3, s);
+      cudaMemcpyAsync(hout.data(), pOut, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf iteration")) || (rc = check_device_error(ctx))) {
+        cleanup();
+        return rc;
+      }
+      ms_fock += elapsed(ctx->ev0, ctx->ev2);
+      auto tb = now();
+      t_build += msec(ta, tb);
+      E = hout[0] + e_nuc;
+      err = hout[1];
+      if (result->history_len < 128) {
+        result->history_energy[result->history_len] = E;
+        result->history_diis_err[result->history_len] = err;
+        result->history_mixed[result->history_len] = prec == RIJK_PREC_MIXED ? 1 : 0;
+        ++result->history_len;
+      }
+      bool stalled = false;
+      if (prec == RIJK_PREC_MIXED) {
+        if (err < best_err * 0.9) {
+          best_err = err;
+          since_best = 0;
+        } else {
+          ++since_best;
+        }
+        // the split-BF16 rounding noise can put a floor under the DIIS error: stop waiting for it
+        stalled = since_best >= 5 || nmix >= o.max_iter / 2;
+      }
+      if (prec == RIJK_PREC_MIXED && (err < o.switch_diis_err || stalled)) {
+        prec = RIJK_PREC_FP64;
+        if (hybrid) {
+          // to the SOSCF loop, which rebuilds F in FP64 for this density.  It needs every
+          // orbital: those of the extrapolated matrix this density came from (or, before the
+          // first extrapolation, the full set of the start)
+          if (have_fex) {
+            auto tc = now();
+            if (diag(pFex, true) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
+            density(pD);
+            t_diag += msec(tc, now());
+          }
+          soscf_from_diis = true;
+          run_soscf = true;
+          it_used = it;
+          break;
+        }
+        // switch to the FP64 form: rebuild F for this same density and restart DIIS (unless the
+        // caller keeps the mixed-phase vectors)
+        if (!o.diis_keep_on_switch) {
+          m = 0;
+          head = 0;
+        }
+        --it;
+        continue;
+      }
+      m = m < m_max ? m + 1 : m_max;
+      head = (head + 1) % m_max;
+      // Pulay B matrix over the stored error vectors
+      std::vector<double> Bm(static_cast<size_t>(m) * m);
+      {
+        int slots[32];
+        for (int i = 0; i < m; ++i) slots[i] = (head - m + i + m_max) % m_max;
+        for (int i = 0; i < m; ++i)
+          for (int j = 0; j <= i; ++j)
+            reduce(DotF{rE + static_cast<size_t>(slots[i]) * nn, rE + static_cast<size_t>(slots[j]) * nn}, nm * nm, 0,
+                   2 + i * (i + 1) / 2 + j);
+        std::vector<double> tmp(kOutSlots);
+        cudaMemcpyAsync(tmp.data(), pOut, kOutSlots * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf DIIS"))) {
+          cleanup();
+          return rc;
+        }
+        for (int i = 0; i < m; ++i)
+          for (int j = 0; j <= i; ++j) Bm[i * m + j] = Bm[j * m + i] = tmp[2 + i * (i + 1) / 2 + j];
+        std::vector<double> c;
+        if (!diis_coefficients(Bm, m, c)) {
+          c.assign(m, 0.0);
+          c[m - 1] = 1.0;
+        }
+        for (int i = 0; i < m; ++i)
+          k_axpy_set<<<grid_of(nn), 256, 0, s>>>(c[i], rF + static_cast<size_t>(slots[i]) * nn, nn, pFex, i == 0);
+      }
+      auto tc = now();
+      t_diis += msec(tb, tc);
+      if (diag(pFex) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
+      have_fex = true;
+      density(pDn);
+      reduce(DiffSqF{pDn, pD}, nn, 0, 0);
+      cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
+      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf density"))) {
+        cleanup();
+        return rc;
+      }
+      rms = std::sqrt(hout[0] / static_cast<double>(nn));
+      t_diag += msec(tc, now());
+      std::swap(pD, pDn);
+      if (rms < o.conv_dm_rms && prec == RIJK_PREC_FP64) {
+        converged = true;
+        break;
+      }
+    }
+  }
+  if (run_soscf) {
     // the reference's RHF iteration (src/SCF.cpp:125-174) with its SOSCF engine
     const long nv = nm - nocc, dim = nocc * nv, dimc = std::max<long>(dim, 1);
     const int mvec = o.lbfgs_vectors > 0 ? o.lbfgs_vectors
@@ -531,13 +657,14 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       return fail(code, msg);
     };
     const unsigned gd = grid_of(dim);
-    const bool guess_diag = o.guess_dm && o.guess_rows && o.guess_nrows > 0;
+    // no first-iteration diagonalisation after a start from a Fock matrix's own orbitals
+    const bool guess_diag = soscf_from_diis || (o.guess_dm && o.guess_rows && o.guess_nrows > 0);
     const double eps = std::numeric_limits<double>::epsilon();
     std::vector<double> rho(mvec, 0.0);
     double E_old = 1e15;
     int step_num = 0, pair_num = 0;
     bool have_rms = false;
-    for (int it = 0; it < o.max_iter; ++it) {
+    for (int it = 0; it < o.max_iter - it_used; ++it) {
       auto ta = now();
       if ((rc = build(prec))) {
         release(lb);
@@ -654,129 +781,34 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     }
     release(lb);
     release(qrw);
-  } else {
-    for (int it = 0; it < o.max_iter; ++it) {
-      auto ta = now();
-      if ((rc = build(prec))) {
-        cleanup();
-        return rc;
-      }
-      // energy and DIIS error X^T (F D S - S D F) X
-      reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
-      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pF, ni, pD, ni, &zero, pT1, ni);   // F D
-      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ni, ni, &one, pT1, ni, pS, ni, &zero, pT2, ni);  // F D S
-      k_antisym<<<grid_of(nn), 256, 0, s>>>(pT2, n, pT1);                                            // FDS - SDF
-      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, pT1, ni, pX, ni, &zero, pT2, ni);  // e X
-      double* slotE = rE + static_cast<size_t>(head) * nn;
-      double* slotF = rF + static_cast<size_t>(head) * nn;
-      cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT2, ni, &zero, slotE, nmi);  // X^T e X
-      cudaMemcpyAsync(slotF, pF, b_nn, cudaMemcpyDeviceToDevice, s);
-      reduce(AbsF{slotE}, nm * nm, 1, 1);
-      cudaEventRecord(ctx->ev3, s);
-      cudaMemcpyAsync(hout.data(), pOut, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
-      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf iteration")) || (rc = check_device_error(ctx))) {
-        cleanup();
-        return rc;
-      }
-      ms_fock += elapsed(ctx->ev0, ctx->ev2);
-      auto tb = now();
-      t_build += msec(ta, tb);
-      E = hout[0] + e_nuc;
-      err = hout[1];
-      if (result->history_len < 128) {
-        result->history_energy[result->history_len] = E;
-        result->history_diis_err[result->history_len] = err;
-        result->history_mixed[result->history_len] = prec == RIJK_PREC_MIXED ? 1 : 0;
-        ++result->history_len;
-      }
-      bool stalled = false;
-      if (prec == RIJK_PREC_MIXED) {
-        if (err < best_err * 0.9) {
-          best_err = err;
-          since_best = 0;
-        } else {
-          ++since_best;
-        }
-        // the split-BF16 rounding noise can put a floor under the DIIS error: stop waiting for it
-        stalled = since_best >= 5 || nmix >= o.max_iter / 2;
-      }
-      if (prec == RIJK_PREC_MIXED && (err < o.switch_diis_err || stalled)) {
-        // switch to the FP64 form: rebuild F for this same density and restart DIIS (unless the
-        // caller keeps the mixed-phase vectors)
-        prec = RIJK_PREC_FP64;
-        if (!o.diis_keep_on_switch) {
-          m = 0;
-          head = 0;
-        }
-        --it;
-        continue;
-      }
-      m = m < m_max ? m + 1 : m_max;
-      head = (head + 1) % m_max;
-      // Pulay B matrix over the stored error vectors
-      std::vector<double> Bm(static_cast<size_t>(m) * m);
-      {
-        int slots[32];
-        for (int i = 0; i < m; ++i) slots[i] = (head - m + i + m_max) % m_max;
-        for (int i = 0; i < m; ++i)
-          for (int j = 0; j <= i; ++j)
-            reduce(DotF{rE + static_cast<size_t>(slots[i]) * nn, rE + static_cast<size_t>(slots[j]) * nn}, nm * nm, 0,
-                   2 + i * (i + 1) / 2 + j);
-        std::vector<double> tmp(kOutSlots);
-        cudaMemcpyAsync(tmp.data(), pOut, kOutSlots * sizeof(double), cudaMemcpyDeviceToHost, s);
-        if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf DIIS"))) {
-          cleanup();
-          return rc;
-        }
-        for (int i = 0; i < m; ++i)
-          for (int j = 0; j <= i; ++j) Bm[i * m + j] = Bm[j * m + i] = tmp[2 + i * (i + 1) / 2 + j];
-        std::vector<double> c;
-        if (!diis_coefficients(Bm, m, c)) {
-          c.assign(m, 0.0);
-          c[m - 1] = 1.0;
-        }
-        for (int i = 0; i < m; ++i)
-          k_axpy_set<<<grid_of(nn), 256, 0, s>>>(c[i], rF + static_cast<size_t>(slots[i]) * nn, nn, pFex, i == 0);
-      }
-      auto tc = now();
-      t_diis += msec(tb, tc);
-      if (diag(pFex) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
-      density(pDn);
-      reduce(DiffSqF{pDn, pD}, nn, 0, 0);
-      cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
-      if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf density"))) {
-        cleanup();
-        return rc;
-      }
-      rms = std::sqrt(hout[0] / static_cast<double>(nn));
-      t_diag += msec(tc, now());
-      std::swap(pD, pDn);
-      if (rms < o.conv_dm_rms && prec == RIJK_PREC_FP64) {
-        converged = true;
-        break;
-      }
+  }
+  // The energy is the last FP64 build's, as the reference reports it (src/SCF.cpp:134-156): a run
+  // that ended in the mixed phase gets one FP64 build at its density for it.
+  if (last_prec != RIJK_PREC_FP64) {
+    if ((rc = build(RIJK_PREC_FP64))) {
+      cleanup();
+      return rc;
     }
+    reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
+    cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf final")) || (rc = check_device_error(ctx))) {
+      cleanup();
+      return rc;
+    }
+    ms_fock += elapsed(ctx->ev0, ctx->ev2);
+    E = hout[0] + e_nuc;
   }
-  // final FP64 build at the converged density: the energy reported is consistent with D
-  if ((rc = build(RIJK_PREC_FP64))) {
-    cleanup();
-    return rc;
-  }
-  reduce(EnergyF{pD, pF, pH}, nn, 0, 0);
-  cudaMemcpyAsync(hout.data(), pOut, sizeof(double), cudaMemcpyDeviceToHost, s);
   if (MO) {
-    // orbitals of the final Fock matrix (all of them), as the reference's closing diagonalisation
+    // every orbital of the last Fock matrix, as the reference's closing diagonalisation
     // (src/SCF.cpp:178)
     if (diag(pF, true) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the final Fock matrix failed");
     cudaMemcpyAsync(MO, pC, static_cast<size_t>(nm) * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf orbitals"))) {
+      cleanup();
+      return rc;
+    }
   }
-  if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf final")) || (rc = check_device_error(ctx))) {
-    cleanup();
-    return rc;
-  }
-  ms_fock += elapsed(ctx->ev0, ctx->ev2);
   if (MO && nm < n) std::memset(MO + nm * n, 0, static_cast<size_t>(n - nm) * n * sizeof(double));
-  E = hout[0] + e_nuc;
   result->energy = E;
   result->dm_rms = rms;
   result->diis_err = err;

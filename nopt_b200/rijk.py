@@ -25,7 +25,7 @@ ERR_ARG, ERR_STATE, ERR_CUDA, ERR_ALLOC, ERR_SOLVER, ERR_TIMEOUT, ERR_NUMERIC, E
 METRIC_INVSQRT, METRIC_CHOLESKY = 0, 1
 LAYOUT_NOPT_FULL, LAYOUT_PACKED = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
-CONV_DIIS, CONV_SOSCF = 0, 1
+CONV_DIIS, CONV_SOSCF, CONV_DIIS_SOSCF = 0, 1, 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -279,8 +279,9 @@ class FockBuilder:
             diis_size=8, guess=None, diis_keep_on_switch=False, converger=CONV_DIIS, conv_grad=1e-7,
             conv_energy=1e-10, lbfgs_vectors=0):
         """RHF on the GPU (rijk_scf); guess = (D0, R) with D0 = R^T R (e.g. SystemIntegrals.sad()),
-        None for the core-Hamiltonian start; converger CONV_DIIS or CONV_SOSCF (the reference's
-        L-BFGS orbital rotations, converged on max|4 F_ai| < conv_grad or |dE| < conv_energy).
+        None for the core-Hamiltonian start; converger CONV_DIIS, CONV_SOSCF (the reference's
+        L-BFGS orbital rotations, converged on max|4 F_ai| < conv_grad or |dE| < conv_energy), or
+        CONV_DIIS_SOSCF (DIIS while the builds are mixed, SOSCF from the switch to FP64 on).
         Returns (E, MO rows, result dict)."""
         n = self.n
         o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1 if diis_keep_on_switch else 0,

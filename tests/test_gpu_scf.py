@@ -118,3 +118,29 @@ def test_gpu_soscf_sad_and_mixed_reach_the_diis_energy():
     assert abs(Es - Ed) < 1e-8 and abs(Em - Ed) < 1e-8, (Ed, Es, Em)
     assert rm["iterations_mixed"] > 0
     assert rs["diis_err"] < 1e-7 or abs(rs["history"][-1][0] - rs["history"][-2][0]) < 1e-10
+
+
+@pytest.mark.parametrize("start", ["sad", "core"])
+def test_gpu_scf_diis_then_soscf(start):
+    """RIJK_CONV_DIIS_SOSCF: DIIS over mixed builds, then from the switch on the reference's SOSCF
+    step over FP64 builds, started from every orbital of the extrapolated Fock matrix the density
+    came from.  It reaches the FP64 DIIS energy to 1e-8 Eh; with FP64 builds throughout it is DIIS."""
+    si = ints.SystemIntegrals(water_cluster((2, 3), seed=2), "cc-pvdz", "cc-pvdz-jkfit")
+    guess = si.sad() if start == "sad" else None
+    with rijk.FockBuilder(0) as fb:
+        fb.set_metric(si.V)
+        fb.set_3c(si.I3, si.n)
+        Ed, _, rd = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess)
+        E64, _, r64 = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess, converger=rijk.CONV_DIIS_SOSCF)
+        Eh, MO, rh = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess, converger=rijk.CONV_DIIS_SOSCF,
+                            precision=rijk.PREC_MIXED)
+    assert rd["converged"] and r64["converged"] and rh["converged"]
+    assert E64 == Ed and r64["iterations"] == rd["iterations"]
+    assert abs(Eh - Ed) < 1e-8, (Ed, Eh)
+    h = rh["history"]
+    nmix = rh["iterations_mixed"]
+    assert nmix > 0 and all(x[2] == 1 for x in h[:nmix]) and all(x[2] == 0 for x in h[nmix:])
+    # the SOSCF phase ends on its own test: max |4 F_ai| < 1e-7 or |dE| < 1e-10
+    assert h[-1][1] < 1e-7 or abs(h[-1][0] - h[-2][0]) < 1e-10
+    C = MO[:rh["nmo"]]
+    assert np.max(np.abs(C @ si.S @ C.T - np.eye(rh["nmo"]))) < 1e-9
