@@ -371,6 +371,10 @@ struct DevBasis {
   const double* coefs = nullptr;
 };
 
+// Every upload goes through the context's stream (cudaMemcpyAsync; pageable sources are staged
+// before the call returns).  That stream is non-blocking: a plain cudaMemcpy, on the legacy
+// stream, would not order against the kernels that read the data and may still be in flight
+// when they start.
 int upload_basis(rijk_ctx* ctx, const HostBasis& h, DevBasis& d) {
   const size_t b0 = h.sh.size() * sizeof(EriShell), b1 = h.exps.size() * sizeof(double);
   std::vector<char> blob(b0 + 2 * b1);
@@ -381,7 +385,8 @@ int upload_basis(rijk_ctx* ctx, const HostBasis& h, DevBasis& d) {
             blob.data() + b0 + b1);
   int rc = ensure(ctx, d.buf, blob.size(), "basis");
   if (rc) return rc;
-  rc = cuda_check(ctx, cudaMemcpy(d.buf.p, blob.data(), blob.size(), cudaMemcpyHostToDevice), "H2D basis");
+  rc = cuda_check(ctx, cudaMemcpyAsync(d.buf.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->stream),
+                  "H2D basis");
   if (rc) return rc;
   char* p = static_cast<char*>(d.buf.p);
   d.sh = reinterpret_cast<const EriShell*>(p);
@@ -484,7 +489,8 @@ int ensure_tables(rijk_ctx* ctx, DevTables& dt) {
           cart[l * 16 + gto_tab::cart_index(l, lx, ly)] = lx | (ly << 4) | ((l - lx - ly) << 8);
     int rc = ensure(ctx, ctx->eri_tab, lay.total, "integral tables");
     if (rc) return rc;
-    rc = cuda_check(ctx, cudaMemcpy(ctx->eri_tab.p, blob.data(), lay.total, cudaMemcpyHostToDevice), "H2D tables");
+    rc = cuda_check(ctx, cudaMemcpyAsync(ctx->eri_tab.p, blob.data(), lay.total, cudaMemcpyHostToDevice, ctx->stream),
+                    "H2D tables");
     if (rc) return rc;
   }
   const char* p = static_cast<const char*>(ctx->eri_tab.p);
@@ -646,8 +652,8 @@ int make_plan(rijk_ctx* ctx, const rijk_basis_t* orb, const rijk_basis_t* aux, E
   if (orb && (rc = upload_basis(ctx, p.orb, p.dorb))) return rc;
   p.kets = ket_lists(p.aux);
   if ((rc = ensure(ctx, p.kets_dev, p.kets.idx.size() * sizeof(int), "ket list"))) return rc;
-  if ((rc = cuda_check(ctx, cudaMemcpy(p.kets_dev.p, p.kets.idx.data(), p.kets.idx.size() * sizeof(int),
-                                       cudaMemcpyHostToDevice), "H2D ket list")))
+  if ((rc = cuda_check(ctx, cudaMemcpyAsync(p.kets_dev.p, p.kets.idx.data(), p.kets.idx.size() * sizeof(int),
+                                            cudaMemcpyHostToDevice, ctx->stream), "H2D ket list")))
     return rc;
   if (orb) {
     const int ns = static_cast<int>(p.orb.sh.size());
@@ -672,8 +678,8 @@ int eri2c_device(rijk_ctx* ctx, EriPlan& p, double* dV, long ld, int* launches) 
   DeviceBuf dp;
   int rc = ensure(ctx, dp, pl.pairs.size() * sizeof(int2), "2c pair list");
   if (rc) return rc;
-  rc = cuda_check(ctx, cudaMemcpy(dp.p, pl.pairs.data(), pl.pairs.size() * sizeof(int2), cudaMemcpyHostToDevice),
-                  "H2D 2c pairs");
+  rc = cuda_check(ctx, cudaMemcpyAsync(dp.p, pl.pairs.data(), pl.pairs.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                                       ctx->stream), "H2D 2c pairs");
   if (!rc) {
     EriLaunch P = base_launch(p.tab);
     P.bra = p.dauxu.sh;
@@ -689,6 +695,7 @@ int eri2c_device(rijk_ctx* ctx, EriPlan& p, double* dV, long ld, int* launches) 
                         launches);
     if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "two-centre integrals");
   }
+  cudaStreamSynchronize(ctx->stream);  // no launch may still read the pair list
   release(dp);
   return rc;
 }
@@ -706,8 +713,8 @@ int eri3c_rows(rijk_ctx* ctx, EriPlan& p, int layout, long mu0, long mu1, long r
   else
     pair_lists(sh, p.orb_pairs, [&](const int2& pr) { return hits(pr.x) || hits(pr.y); }, pl);
   if (pl.pairs.empty()) return RIJK_OK;
-  int rc = cuda_check(ctx, cudaMemcpy(p.pairs_dev.p, pl.pairs.data(), pl.pairs.size() * sizeof(int2),
-                                      cudaMemcpyHostToDevice), "H2D 3c pairs");
+  int rc = cuda_check(ctx, cudaMemcpyAsync(p.pairs_dev.p, pl.pairs.data(), pl.pairs.size() * sizeof(int2),
+                                           cudaMemcpyHostToDevice, ctx->stream), "H2D 3c pairs");
   if (rc) return rc;
   EriLaunch P = base_launch(p.tab);
   P.bra = p.dorb.sh;

@@ -42,7 +42,11 @@ int cuda_check(rijk_ctx* ctx, cudaError_t e, const char* what) {
 
 int ensure(rijk_ctx* ctx, DeviceBuf& b, size_t bytes, const char* what) {
   if (b.bytes >= bytes && b.p) return RIJK_OK;
-  if (b.p) cudaFree(b.p);
+  if (b.p) {  // the old buffer may still be read by work queued on the context's streams
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    cudaFree(b.p);
+  }
   b.p = nullptr;
   b.bytes = 0;
   if (bytes == 0) return RIJK_OK;
@@ -254,7 +258,8 @@ RIJK_API int rijk_create(rijk_ctx** out, int device) {
     rijk_destroy(ctx);
     return RIJK_ERR_ALLOC;
   }
-  cudaMemset(ctx->err.p, 0, sizeof(int));
+  cudaMemsetAsync(ctx->err.p, 0, sizeof(int), ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
   *out = ctx;
   return RIJK_OK;
 }
@@ -263,6 +268,7 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
   if (!ctx) return RIJK_ERR_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // before any buffer it may touch is freed
   DeviceBuf* bufs[] = {&ctx->M, &ctx->B, &ctx->Bmix, &ctx->stageD, &ctx->stageMO, &ctx->stageJ, &ctx->stageK,
                        &ctx->Dt, &ctx->w, &ctx->Jpart, &ctx->MOp, &ctx->XT, &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab};
   for (DeviceBuf* b : bufs) release(*b);
@@ -286,10 +292,8 @@ RIJK_API int rijk_set_stream(rijk_ctx* ctx, void* stream) {
   if (!ctx) return RIJK_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (ctx->own_stream && ctx->stream) {
-    cudaStreamSynchronize(ctx->stream);
-    cudaStreamDestroy(ctx->stream);
-  }
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);  // work queued on the old stream ends first
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   ctx->stream = s;
   ctx->own_stream = false;
   cublasSetStream(ctx->cublas, s);
@@ -542,7 +546,7 @@ int check_device_error(rijk_ctx* ctx) {
   int rc = cuda_check(ctx, cudaMemcpy(&h, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost), "error word");
   if (rc) return rc;
   if (h == 0) return RIJK_OK;
-  cudaMemset(ctx->err.p, 0, sizeof(int));
+  cudaMemsetAsync(ctx->err.p, 0, sizeof(int), ctx->stream);  // ordered before the next launch
   if (h & DEVERR_TIMEOUT) return set_err(ctx, RIJK_ERR_TIMEOUT, "a device-side wait ran out (error bits 0x%x)", h);
   if (h & DEVERR_NAN) return set_err(ctx, RIJK_ERR_NUMERIC, "non-finite value detected (error bits 0x%x)", h);
   return set_err(ctx, RIJK_ERR_CUDA, "device error bits 0x%x", h);
