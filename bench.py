@@ -496,6 +496,24 @@ def main():
     except rijk.RijkError as e:
         mixed = {"unavailable": str(e)}
 
+    # the FP64 form with K on tcgen05 tensor cores from int8 digit planes (RIJK_PREC_FP64_TC, opt-in)
+    fp64tc = None
+    if not sharded:
+        try:
+            mst = timed(rijk.PREC_FP64_TC, args.steps, 3)
+            fb.sync()
+            Kt = dK.cpu().numpy().copy()
+            fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), rijk.PREC_FP64)
+            fb.sync()
+            K64t = dK.cpu().numpy()
+            fp64tc = {"value": 1e3 / mst, "unit": "builds/s", "ms_per_step": mst, "speedup_vs_fp64": ms / mst,
+                      "max_abs_dK_vs_fp64": float(np.max(np.abs(Kt - K64t))),
+                      "stage_ms": stage_times(rijk.PREC_FP64_TC),
+                      "note": "syrk_i8 = the int8 digit planes of X^T plus K from 36 exact s32 digit products; "
+                              "J and the half-transform as the FP64 form"}
+        except rijk.RijkError as e:
+            fp64tc = {"unavailable": str(e)}
+
     # per-iteration errors of the mixed form along an FP64 SCF path: at each iteration's density both
     # forms are built; max |dJ|, max |dK| and the energy difference tr((2 dJ - dK) D) are recorded
     if isinstance(mixed, dict) and "unavailable" not in mixed and not sharded and not synthetic:
@@ -588,7 +606,7 @@ def main():
                        "h2d_bytes_per_step": int((n * n + nocc * n) * 8), "d2h_bytes_per_step": int(2 * n * n * 8)},
                "gpu_launches": launches,
                "roofline": roof, "coulomb_roofline": coul, "stage_ms": stage_ms,
-               "mixed": mixed, "scf": scf, "cpu_baseline": cpu, "clocks": clk.summary(),
+               "mixed": mixed, "fp64_tc": fp64tc, "scf": scf, "cpu_baseline": cpu, "clocks": clk.summary(),
                "setup": {"path": "rijk_set_basis (GPU integrals)" if args.setup == "gpu" else "host integrals + rijk_set_3c",
                          "wall_s": t_setup,
                          "gpu_integrals_ms": st0["ms_setup_ints"] if args.setup == "gpu" else None,

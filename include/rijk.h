@@ -57,6 +57,10 @@ extern "C" {
 #define RIJK_PREC_FP64 0  /* FP64 throughout: the drop-in form                                   */
 #define RIJK_PREC_MIXED 1 /* exchange half-transform and K on tcgen05 tensor cores with split-BF16
                              (3-term) operands and FP32 accumulation; Coulomb in FP64          */
+#define RIJK_PREC_FP64_TC 2 /* FP64 results, with K = X^T X on tcgen05 tensor cores: X^T split
+                             into 8 int8 digit planes per row and split-K part (a power-of-two
+                             exponent each), 36 exact s32 digit products, FP64 scaling and sums
+                             (the Ozaki splitting scheme); J and the half-transform as FP64   */
 
 typedef struct rijk_ctx rijk_ctx;
 

@@ -24,6 +24,7 @@ CUDA_SOURCES = [
     "rijk/k_coulomb.cu",
     "rijk/k_exchange_f64.cu",
     "rijk/k_exchange_tc.cu",
+    "rijk/k_exchange_i8.cu",
     "rijk/k_scf.cu",
     "rijk/k_adjoint.cu",
     "rijk/k_moints.cu",

@@ -186,7 +186,9 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
   } else {
     const long noccp = round_up(nocc, 16);
     const long kdim = naux * noccp;
-    const int nsK = syrk_nsplit(nt, kdim);
+    const bool tc = precision == RIJK_PREC_FP64_TC;
+    long kper_tc = 0;
+    const int nsK = tc ? syrk_i8_parts(nt, kdim, ctx->device, &kper_tc) : syrk_nsplit(nt, kdim);
     if ((rc = ensure(ctx, ctx->MOp, noccp * npad * sizeof(double), "MOp")) ||
         (rc = ensure(ctx, ctx->XT, static_cast<size_t>(npad) * kdim * sizeof(double), "XT")) ||
         (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(nsK) * tile_elems * sizeof(double), "Kpart")))
@@ -196,9 +198,17 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
     launch_xform_f64(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->MOp.p), naux, nt, noccp,
                      static_cast<double*>(ctx->XT.p), s);
     prof_mark(ctx, "xform_f64");
-    launch_syrk_f64(static_cast<const double*>(ctx->XT.p), npad, nt, kdim, nsK, static_cast<double*>(ctx->Kpart.p),
-                    s);
-    prof_mark(ctx, "syrk_f64");
+    if (tc) {  // int8 digit planes of X^T, then K on tcgen05 (exact s32 products)
+      rc = syrk_i8(ctx, static_cast<const double*>(ctx->XT.p), npad, nt, kdim, nsK, kper_tc,
+                   static_cast<double*>(ctx->Kpart.p), s);
+      if (rc) return rc;
+      prof_mark(ctx, "syrk_i8");
+      ++launches;  // the digit-plane pass
+    } else {
+      launch_syrk_f64(static_cast<const double*>(ctx->XT.p), npad, nt, kdim, nsK, static_cast<double*>(ctx->Kpart.p),
+                      s);
+      prof_mark(ctx, "syrk_f64");
+    }
     launch_unpack_sym(static_cast<double*>(ctx->Kpart.p), nsK, ntile, n, dK, s);
     prof_mark(ctx, "unpack_k");
     launches += 4;
@@ -269,8 +279,9 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // before any buffer it may touch is freed
-  DeviceBuf* bufs[] = {&ctx->M, &ctx->B, &ctx->Bmix, &ctx->stageD, &ctx->stageMO, &ctx->stageJ, &ctx->stageK,
-                       &ctx->Dt, &ctx->w, &ctx->Jpart, &ctx->MOp, &ctx->XT, &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab};
+  DeviceBuf* bufs[] = {&ctx->M,  &ctx->B,     &ctx->Bmix,  &ctx->stageD, &ctx->stageMO, &ctx->stageJ,
+                       &ctx->stageK, &ctx->Dt, &ctx->w,     &ctx->Jpart, &ctx->MOp,    &ctx->XT,
+                       &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab, &ctx->Xs, &ctx->Xe};
   for (DeviceBuf* b : bufs) release(*b);
   if (ctx->cublas) cublasDestroy(ctx->cublas);
   if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
@@ -571,7 +582,7 @@ int check_fock_args(rijk_ctx* ctx, long nocc, int precision) {
   if (!ctx->have_b) return set_err(ctx, RIJK_ERR_STATE, "Fock build before rijk_set_3c");
   if (nocc < 0 || nocc > round_up(ctx->n, 16))
     return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld outside [0, n_ao = %ld]", nocc, ctx->n);
-  if (precision != RIJK_PREC_FP64 && precision != RIJK_PREC_MIXED)
+  if (precision != RIJK_PREC_FP64 && precision != RIJK_PREC_MIXED && precision != RIJK_PREC_FP64_TC)
     return set_err(ctx, RIJK_ERR_ARG, "unknown precision %d", precision);
   // the FP64 half-transform runs in orbital batches (any n_c); the tcgen05 form holds all n_c
   // columns of one aux function in TMEM (N <= 192)

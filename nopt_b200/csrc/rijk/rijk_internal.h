@@ -75,6 +75,9 @@ struct rijk_ctx {
   rijk::DeviceBuf err;    // int device error word
   rijk::DeviceBuf scratch;  // misc small
   rijk::DeviceBuf eri_tab;  // integral tables (Boys grid, harmonics, aux term lists)
+  rijk::DeviceBuf Xs;       // int8 digits of X^T for the tensor-core FP64 exchange: npad2 rows of kdim/32
+                            // blocks of 8 digits x 32 bytes
+  rijk::DeviceBuf Xe;       // their row exponents, parts x npad2
 
   rijk_stats_t stats{};
   std::string last_error;
@@ -146,5 +149,10 @@ void launch_coulomb_j_mixed(const __nv_bfloat16* Bmix, const double* w, long nau
 void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s);
 int syrk_nsplit(long nt, long kdim);
 void launch_syrk_f64(const double* XT, long npad, long nt, long kdim, int nsplit, double* Kpart, cudaStream_t s);
+
+// ---- k_exchange_i8.cu (RIJK_PREC_FP64_TC): K partials from int8 digit planes on tcgen05
+int syrk_i8_parts(long nt, long kdim, int device, long* kper);
+int syrk_i8(rijk_ctx* ctx, const double* XT, long npad, long nt, long kdim, int nparts, long kper, double* Kpart,
+            cudaStream_t s);
 
 }  // namespace rijk

@@ -158,6 +158,31 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr, uint64_t bits) {
   return bits | static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
 }
 
+// Descriptor bits of a K-major operand with 32-byte swizzle (layout code 6): 8-row x 32-byte
+// atoms, SBO = 256 B between atoms.  One atom row holds the 32 int8 K-elements of one kind::i8 MMA.
+__host__ __device__ constexpr uint64_t sw32_desc_bits(uint32_t sbo_bytes) {
+  return (static_cast<uint64_t>(1) << 16) | (static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFF) << 32) | (1ULL << 46) |
+         (6ULL << 61);
+}
+
+// Instruction descriptor of kind::i8: D s32 (bits 4-5 = 2), A and B signed 8-bit (bits 7-9 and
+// 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+         (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+// D (s32, TMEM) (+)= A (s8) . B (s8), exact integer products and sums.
+__device__ __forceinline__ void umma_s8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, int a_mn_major, int b_mn_major) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(a_mn_major) << 15) |
          (static_cast<uint32_t>(b_mn_major) << 16) | (static_cast<uint32_t>(N >> 3) << 17) |

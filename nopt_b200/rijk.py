@@ -24,7 +24,7 @@ OK = 0
 ERR_ARG, ERR_STATE, ERR_CUDA, ERR_ALLOC, ERR_SOLVER, ERR_TIMEOUT, ERR_NUMERIC, ERR_CONVERGE = -1, -2, -3, -4, -5, -6, -7, -8
 METRIC_INVSQRT, METRIC_CHOLESKY = 0, 1
 LAYOUT_NOPT_FULL, LAYOUT_PACKED = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP64_TC = 0, 1, 2
 CONV_DIIS, CONV_SOSCF, CONV_DIIS_SOSCF = 0, 1, 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
