@@ -311,6 +311,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   cublasHandle_t cb = ctx->cublas;
   cusolverDnHandle_t cs = ctx->cusolver;
   const int m_max = o.diis_size;
+  constexpr long kMixedRows = 192;  // orbitals one mixed build takes
 
   DeviceBuf dH, dS, dX, dF, dFex, dD, dDn, dC, dJ, dK, dT1, dT2, dE, dW, dU, work, info, red, out, ring_F, ring_E;
   auto cleanup = [&]() {
@@ -452,7 +453,19 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     cudaMemcpyAsync(pD, o.guess_dm, b_nn, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dR.p, o.guess_rows, static_cast<size_t>(o.guess_nrows) * n * sizeof(double),
                     cudaMemcpyHostToDevice, s);
-    rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, RIJK_PREC_FP64);
+    // The guess Fock matrix only seeds the first diagonalisation: a mixed run builds it in the
+    // mixed form, K summed over batches of at most 192 factor rows (K is linear in D = R^T R).
+    if (o.precision == RIJK_PREC_MIXED) {
+      const long nr = o.guess_nrows;
+      const double* R = static_cast<const double*>(dR.p);
+      for (long r0 = 0; r0 < nr && !rc; r0 += kMixedRows) {
+        const long cnt = std::min(kMixedRows, nr - r0);
+        rc = fock_device_impl(ctx, pD, R + r0 * n, cnt, r0 == 0 ? pJ : pT1, r0 == 0 ? pK : pT2, RIJK_PREC_MIXED);
+        if (!rc && r0 > 0) k_axpy_set<<<grid_of(nn), 256, 0, s>>>(1.0, pT2, nn, pK, 0);
+      }
+    } else {
+      rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, RIJK_PREC_FP64);
+    }
     if (!rc) {
       k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
       rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf guess");
