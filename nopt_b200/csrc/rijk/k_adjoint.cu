@@ -285,11 +285,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   }
   double* pGam = static_cast<double*>(Gam.p);
   const size_t gsmem = 4 * 64 * LDK * sizeof(double);
-  static bool gattr = false;
-  if (!gattr) {
-    cudaFuncSetAttribute(k_gamma_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(gsmem));
-    gattr = true;
-  }
+  ensure_smem_limit(reinterpret_cast<const void*>(k_gamma_f64), gsmem);
   const double half = 0.5;
   for (long q0 = 0; q0 < naux; q0 += qc) {
     const long nq = std::min(qc, naux - q0);

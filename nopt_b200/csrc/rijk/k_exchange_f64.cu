@@ -102,11 +102,7 @@ static void launch_xform_nf(const double* B, const double* MOp, long naux, long 
   constexpr int NOCCP = NF * 16;
   constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
   size_t smem = (2 * A_STAGE + 2 * NOCCP * LDK) * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_xform_f64<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attr = true;
-  }
+  ensure_smem_limit(reinterpret_cast<const void*>(k_xform_f64<NF>), smem);
   long npad = nt * TILE;
   long tile_elems = nt * (nt + 1) / 2 * TILE2;
   dim3 grid(static_cast<unsigned>(nt), static_cast<unsigned>(naux));
@@ -199,18 +195,19 @@ constexpr size_t kSyrkSmem = 4 * 64 * LDK * sizeof(double);
 
 // CTAs of k_syrk_f64 resident per SM (registers and shared memory), from the runtime.
 int syrk_ctas_per_sm() {
-  static int per_sm = 0;
-  if (!per_sm) {
-    cudaFuncSetAttribute(k_syrk_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSyrkSmem));
-    int nb = 0;
+  static int slots[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_f64), kSyrkSmem);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (!slots[dev]) {
+    int nb = 0, sms = 148;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_syrk_f64, S_THREADS, kSyrkSmem) != cudaSuccess || nb < 1)
       nb = 2;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    per_sm = nb * sms;  // slots of one wave
+    slots[dev] = nb * sms;  // slots of one wave
   }
-  return per_sm;
+  return slots[dev];
 }
 }  // namespace
 

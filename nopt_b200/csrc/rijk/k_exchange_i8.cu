@@ -427,11 +427,7 @@ int syrk_i8(rijk_ctx* ctx, const double* XT, long npad, long nt, long kdim, int 
   ip.E = E;
   ip.err = static_cast<int*>(ctx->err.p);
   const size_t smem = static_cast<size_t>(ip.stages) * kI8Stage + 1024 + 256;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_syrk_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attr = true;
-  }
+  ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_i8), smem);
   const long nb = npad2 / 128;
   dim3 grid(static_cast<unsigned>(nb * (nb + 1) / 2), static_cast<unsigned>(nparts));
   k_syrk_i8<<<grid, kI8Threads, smem, s>>>(mX, ip);

@@ -805,11 +805,7 @@ void launch_xform_tc(const CUtensorMap& mB, const CUtensorMap& mC, XformParams p
   p.c_resident = sr >= 3 ? 1 : 0;
   p.stages = p.c_resident ? sr : Cfg::stages();
   const size_t smem = p.c_resident ? Cfg::smem_resident(p.stages, p.nt2) : Cfg::smem(p.stages);
-  static size_t attr = 0;
-  if (smem > attr) {
-    cudaFuncSetAttribute(k_xform_tc<NOCCP>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attr = smem;
-  }
+  ensure_smem_limit(reinterpret_cast<const void*>(k_xform_tc<NOCCP>), smem);
   int nitems = p.naux * p.npairs;
   int grid = std::min(nitems, num_sms(device));
   k_xform_tc<NOCCP><<<grid, kTcThreads, smem, s>>>(mB, mC, p);
@@ -942,11 +938,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
     pp.seg = kSySeg;
     pp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
     const size_t smem2 = static_cast<size_t>(pp.stages) * kSyStage + 1024 + 256;
-    static bool attr2 = false;
-    if (!attr2) {
-      cudaFuncSetAttribute(k_syrk_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem2));
-      attr2 = true;
-    }
+    ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_tc2), smem2);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(static_cast<unsigned>(2 * tiles256), static_cast<unsigned>(nsplit2));
     cfg.blockDim = dim3(kPairThreads);
@@ -979,11 +971,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   sp.seg = kSySeg;
   sp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
   size_t smem = static_cast<size_t>(sp.stages) * kSyStage + 1024 + 256;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attr = true;
-  }
+  ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_tc), smem);
   dim3 grid(static_cast<unsigned>(ntile128), static_cast<unsigned>(nsplit));
   k_syrk_tc<<<grid, kTcThreads, smem, s>>>(mX, sp);
   ++launches;

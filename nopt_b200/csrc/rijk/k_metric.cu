@@ -108,11 +108,7 @@ void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const
   long pair_base = mu0 * (mu0 + 1) / 2;
   dim3 grid(static_cast<unsigned>((t1 - t0) * TILE), static_cast<unsigned>((naux + 63) / 64));
   const size_t smem = 4 * 64 * LDK * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_metric_contract, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attr = true;
-  }
+  ensure_smem_limit(reinterpret_cast<const void*>(k_metric_contract), smem);
   k_metric_contract<<<grid, K1_THREADS, smem, s>>>(M, nauxp, mrows, I3, layout, n, naux, I0, t0, pair_base, B,
                                                    ntile * TILE2);
 }

@@ -7,6 +7,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "gemm_f64.cuh"
@@ -54,6 +56,19 @@ int ensure(rijk_ctx* ctx, DeviceBuf& b, size_t bytes, const char* what) {
   if (e != cudaSuccess) return cuda_check(ctx, e, what);
   b.bytes = bytes;
   return RIJK_OK;
+}
+
+cudaError_t ensure_smem_limit(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = done[{fn, dev}];
+  if (have >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  if (e == cudaSuccess) have = bytes;
+  return e;
 }
 
 void release(DeviceBuf& b) {

@@ -101,6 +101,10 @@ int ensure(rijk_ctx* ctx, DeviceBuf& b, size_t bytes, const char* what);
 void release(DeviceBuf& b);
 float elapsed(cudaEvent_t a, cudaEvent_t b);
 int check_device_error(rijk_ctx* ctx);
+// Raises kernel `fn`'s dynamic shared-memory limit to at least `bytes` on the current device.  The
+// attribute lives in each device's context, so it is set once per (kernel, device), not once per
+// process: a process that drives several GPUs sets it on each.
+cudaError_t ensure_smem_limit(const void* fn, size_t bytes);
 int check_fock_args(rijk_ctx* ctx, long nocc, int precision);
 // One Fock build on device pointers (J into dJ, K into dK), asynchronous on ctx->stream.  With
 // mo_ready the exchange waits for that event (dMO is written on another stream); with j_done the
