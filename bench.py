@@ -559,7 +559,7 @@ def main():
                 ("diis_mixed_then_soscf_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF))
         for name, prec, conv in runs:
             el = None
-            for _ in range(2):  # the faster of two runs: host-side latencies make single SCF timings noisy
+            for _ in range(3):  # the fastest of three runs: host-side latencies make single SCF timings noisy
                 torch.cuda.synchronize(dev)
                 t0 = time.perf_counter()
                 E, _, r = fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, conv_dm_rms=1e-10, guess=guess,
@@ -581,7 +581,7 @@ def main():
                             "diis_mixed_then_soscf_fp64: DIIS over the mixed builds, the SOSCF step and test after "
                             "the switch")
         out["start"] = "superposition of atomic densities (%.2f s on the host, not in the SCF time)" % t_guess
-        out["timing"] = ("wall time of rijk_scf, the faster of two runs (ms_inside: the library's own clock of "
+        out["timing"] = ("wall time of rijk_scf, the fastest of three runs (ms_inside: the library's own clock of "
                          "that run, without argument checks and buffer release)")
         scf = out
 
