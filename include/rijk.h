@@ -177,8 +177,9 @@ int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ);
 typedef struct {
   int max_iter;           /* default 100                                                        */
   double conv_dm_rms;     /* converged when RMS(D_new - D) falls below this; default 1e-10     */
-  int precision;          /* RIJK_PREC_FP64, or RIJK_PREC_MIXED: mixed builds until the DIIS
-                             error falls below switch_diis_err, FP64 builds after that        */
+  int precision;          /* RIJK_PREC_FP64 or RIJK_PREC_FP64_TC (FP64 results throughout), or
+                             RIJK_PREC_MIXED: mixed builds until the DIIS error falls below
+                             switch_diis_err, RIJK_PREC_FP64 builds after that                */
   double switch_diis_err; /* default 1e-5; the switch also happens when the mixed-phase error has
                              not improved for 5 iterations or after max_iter / 2 mixed iterations */
   int diis_size;          /* default 8                                                          */

@@ -444,7 +444,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   };
 
   if (o.guess_dm && o.guess_rows && o.guess_nrows > 0) {
-    // start from the given density: one FP64 build with its factor rows, then diagonalise
+    // start from the given density: one build with its factor rows, then diagonalise
     DeviceBuf dR;
     if ((rc = ensure(ctx, dR, static_cast<size_t>(o.guess_nrows) * n * sizeof(double), "scf guess rows"))) {
       cleanup();
@@ -464,7 +464,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
         if (!rc && r0 > 0) k_axpy_set<<<grid_of(nn), 256, 0, s>>>(1.0, pT2, nn, pK, 0);
       }
     } else {
-      rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, RIJK_PREC_FP64);
+      rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, o.precision);
     }
     if (!rc) {
       k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
@@ -619,7 +619,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       rms = std::sqrt(hout[0] / static_cast<double>(nn));
       t_diag += msec(tc, now());
       std::swap(pD, pDn);
-      if (rms < o.conv_dm_rms && prec == RIJK_PREC_FP64) {
+      if (rms < o.conv_dm_rms && prec != RIJK_PREC_MIXED) {  // FP64 results (RIJK_PREC_FP64 or _FP64_TC)
         converged = true;
         break;
       }
@@ -797,7 +797,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   }
   // The energy is the last FP64 build's, as the reference reports it (src/SCF.cpp:134-156): a run
   // that ended in the mixed phase gets one FP64 build at its density for it.
-  if (last_prec != RIJK_PREC_FP64) {
+  if (last_prec == RIJK_PREC_MIXED || last_prec < 0) {
     if ((rc = build(RIJK_PREC_FP64))) {
       cleanup();
       return rc;

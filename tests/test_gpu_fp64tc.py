@@ -70,3 +70,18 @@ def test_fp64tc_k_water_hexamer():
     DM, MO = _state(si.n, si.nocc, 2)
     eK, eKf = _check(si.V, si.I3, si.n, si.nocc, DM, MO)
     assert eK < 1e-11, (eK, eKf)
+
+
+def test_fp64tc_scf_matches_fp64():
+    """rijk_scf with every build in the FP64_TC form (the SAD guess build included) converges to the
+    FP64 energy: the digit form is held to FP64 accuracy, so it converges on the FP64 criteria."""
+    si = ints.SystemIntegrals(water_cluster((2, 3), seed=1), "cc-pvdz", "cc-pvdz-jkfit")
+    guess = si.sad()
+    with rijk.FockBuilder(0) as fb:
+        fb.set_metric(si.V)
+        fb.set_3c(si.I3, si.n)
+        E64, _, r64 = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess)
+        Et, _, rt = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess, precision=rijk.PREC_FP64_TC)
+    assert r64["converged"] and rt["converged"]
+    assert rt["iterations_mixed"] == 0
+    assert abs(Et - E64) < 1e-10, (Et, E64)

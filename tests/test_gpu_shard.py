@@ -1,6 +1,6 @@
 """Aux-index slices on the GPU (rijk_set_aux_range): two contexts holding [0, q1) and
-[q1, naux) give partial J, K and active integrals that sum to the full ones (FP64 to 1e-9,
-mixed to its tolerance).  This is the arithmetic of the multi-GPU sharding in
+[q1, naux) give partial J, K and active integrals that sum to the full ones (FP64 and the
+int8-digit FP64_TC K to 1e-9, mixed to its tolerance).  This is the arithmetic of the multi-GPU sharding in
 nopt_b200.parallel, checked on one GPU without collectives."""
 import numpy as np
 import pytest
@@ -30,12 +30,15 @@ def test_two_aux_slices_sum_to_full():
             Jm, Km = fb.dm_to_f_transform_ri(DM, MO, si.nocc, rijk.PREC_MIXED)
             act = MO[si.nocc - 2:si.nocc + 2]
             I, _, _ = fb.calc_2el_mo_ints_ri(None, MO, act, act, 0, 4, want_jk=False)
-            out[name] = (J, K, Jm, Km, I)
+            _, Kt = fb.dm_to_f_transform_ri(DM, MO, si.nocc, rijk.PREC_FP64_TC)
+            out[name] = (J, K, Jm, Km, I, Kt)
     f, a, b = out["full"], out["a"], out["b"]
     assert np.max(np.abs(a[0] + b[0] - f[0])) < 1e-9
     assert np.max(np.abs(a[1] + b[1] - f[1])) < 1e-9
     assert np.max(np.abs(a[4] + b[4] - f[4])) < 1e-9
     assert np.max(np.abs(a[3] + b[3] - f[1])) < 2e-4
+    # the int8 digit form of K on each slice: digit exponents per slice, FP64 partials that sum
+    assert np.max(np.abs(a[5] + b[5] - f[1])) < 1e-9
     with rijk.FockBuilder(0) as fb:
         fb.set_metric(si.V)
         with pytest.raises(rijk.RijkError) as e:
