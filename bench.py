@@ -510,8 +510,8 @@ def main():
             fp64tc = {"value": 1e3 / mst, "unit": "builds/s", "ms_per_step": mst, "speedup_vs_fp64": ms / mst,
                       "max_abs_dK_vs_fp64": float(np.max(np.abs(Kt - K64t))),
                       "stage_ms": stage_times(rijk.PREC_FP64_TC),
-                      "note": "syrk_i8 = the int8 digit planes of X^T plus K from 36 exact s32 digit products; "
-                              "J and the half-transform as the FP64 form"}
+                      "note": "slice_x = the int8 digits of X^T (8 per element); syrk_i8 = K from 36 exact s32 "
+                              "digit products; J and the half-transform as the FP64 form"}
         except rijk.RijkError as e:
             fp64tc = {"unavailable": str(e)}
 

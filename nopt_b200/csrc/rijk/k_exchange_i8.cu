@@ -9,7 +9,7 @@
 // left after 8 digits is below 2^-57 of the row maximum.  Then
 //     K_mu,nu = 2^(e_mu + e_nu) sum_g 2^{-7(g+2)} sum_{s+t=g} (d_s[mu] . d_t[nu]),
 // where every (d_s . d_t) is an exact s32 tensor-core sum (|d_s d_t| <= 4096; a part spans at
-// most 65536 k, and a group sums at most 8 pairs: 8 * 4096 * 65536 = 2^31).  The groups g < 8
+// most 65504 k, and a group sums at most 8 pairs: 8 * 4096 * 65504 < 2^31 - 1).  The groups g < 8
 // (36 digit pairs) are kept; the dropped ones are below 9 * 2^-58 of 2^(e_mu + e_nu) per k,
 // the level of FP64 rounding in a sum of products.
 //
@@ -49,7 +49,7 @@ constexpr int kI8Threads = 192;                // warp 0 TMA, warp 1 MMA, warps 
 constexpr int kBlock = kDigits * kChunk;       // bytes per row and 32 k: 8 digits x 32 B
 constexpr uint32_t kHalf = 128 * 128;          // 4 digits of a 128-row panel: 128 rows x 128 B
 constexpr uint32_t kI8Stage = 4 * kHalf;       // A digits 0-3, A 4-7, B 0-3, B 4-7: 64 KB
-constexpr long kMaxPart = 65536;               // k per split part that keeps every s32 sum exact
+constexpr long kMaxPart = 65504;               // k per split part: 8 * 4096 * 65504 < 2^31 - 1, every s32 sum exact
 constexpr int kI8SmemBudget = 225 * 1024;
 
 __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
@@ -57,14 +57,12 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 }
 
 // ------------------------------------------------------------------ digit planes ----
-// One CTA per (row nu, part r): the part (at most kMaxSlicePart k) is read once into registers,
-// four consecutive k per thread and step, the CTA takes the row's exponent over the part, and
-// each thread writes its 8 digits of 4 consecutive k as packed 4-byte words into the k's block.
-// Rows at or past npad (the padding of the 128-row blocks), and k from kdim to the end of the
-// last block, get zero digits.
+// One CTA per (row nu, part r), part length up to kMaxPart: a first sweep takes the row's maximum
+// over the part (from HBM), a second one re-reads the part (now in L2) and writes each thread's
+// 8 digits of 4 consecutive k as packed 4-byte words into the k's block.  Rows at or past npad
+// (the padding of the 128-row blocks), and k from kdim to the end of the last block, get zero
+// digits.
 constexpr int kSliceThreads = 256;
-constexpr int kSliceSteps = 8;  // 8 x 256 x 4 = 8192 k per part at most
-constexpr long kMaxSlicePart = static_cast<long>(kSliceSteps) * kSliceThreads * 4;
 
 __global__ void __launch_bounds__(kSliceThreads) k_slice_x(const double* __restrict__ XT, long npad, long npad2,
                                                            long kdim, long kper, int8_t* __restrict__ Xs,
@@ -72,24 +70,19 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_x(const double* __restr
   __shared__ double wmax[kSliceThreads / 32];
   const long row = blockIdx.x, part = blockIdx.y;
   const long k0 = part * kper, k1 = std::min(k0 + kper, kdim);
+  const long kend = k1 == kdim ? (kdim + kChunk - 1) / kChunk * kChunk : k1;  // zero digits fill the last block
   const long nblk = (kdim + kChunk - 1) / kChunk;
   int8_t* out = Xs + static_cast<size_t>(row) * nblk * kBlock;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  double v[kSliceSteps][4];
+  const bool live = row < npad;
+  const double* x = XT + static_cast<size_t>(live ? row : 0) * kdim;
   double m = 0.0;
-  const double* x = XT + static_cast<size_t>(row < npad ? row : 0) * kdim;
-#pragma unroll
-  for (int j = 0; j < kSliceSteps; ++j) {
-    const long k = k0 + 4L * (t + kSliceThreads * j);
-    const bool in = row < npad && k < k1;  // k1 and k are multiples of 4
-    const double2 a = in ? *reinterpret_cast<const double2*>(x + k) : make_double2(0.0, 0.0);
-    const double2 b = in ? *reinterpret_cast<const double2*>(x + k + 2) : make_double2(0.0, 0.0);
-    v[j][0] = a.x;
-    v[j][1] = a.y;
-    v[j][2] = b.x;
-    v[j][3] = b.y;
-    m = fmax(m, fmax(fmax(fabs(a.x), fabs(a.y)), fmax(fabs(b.x), fabs(b.y))));
-  }
+  if (live)
+    for (long k = k0 + 4L * t; k < k1; k += 4L * kSliceThreads) {  // k1 and k are multiples of 4
+      const double2 a = *reinterpret_cast<const double2*>(x + k);
+      const double2 b = *reinterpret_cast<const double2*>(x + k + 2);
+      m = fmax(m, fmax(fmax(fabs(a.x), fabs(a.y)), fmax(fabs(b.x), fabs(b.y))));
+    }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (lane == 0) wmax[warp] = m;
@@ -100,15 +93,20 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_x(const double* __restr
   // m = f 2^(b+1) with f in [1/2, 1) (b = ilogb(m)); dividing by 2^(b+2) leaves |x| < 1/2
   const int e = m > 0.0 ? ilogb(m) + 2 : 0;
   if (t == 0) E[part * npad2 + row] = e;
-  const long kend = k1 == kdim ? (kdim + kChunk - 1) / kChunk * kChunk : k1;  // zero digits fill the last block
-#pragma unroll
-  for (int j = 0; j < kSliceSteps; ++j) {
-    const long k = k0 + 4L * (t + kSliceThreads * j);
-    if (k >= kend) break;
+  for (long k = k0 + 4L * t; k < kend; k += 4L * kSliceThreads) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (live && k < k1) {
+      const double2 a = *reinterpret_cast<const double2*>(x + k);
+      const double2 b = *reinterpret_cast<const double2*>(x + k + 2);
+      v[0] = a.x;
+      v[1] = a.y;
+      v[2] = b.x;
+      v[3] = b.y;
+    }
     uint32_t packed[kDigits] = {};
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      double r = ldexp(v[j][q], -e);
+      double r = ldexp(v[q], -e);
 #pragma unroll
       for (int d = 0; d < kDigits; ++d) {
         const double tt = r * 128.0;
@@ -121,6 +119,11 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_x(const double* __restr
 #pragma unroll
     for (int d = 0; d < kDigits; ++d) *reinterpret_cast<uint32_t*>(blk + d * kChunk) = packed[d];
   }
+}
+
+// 2^e exactly for |e| <= 1000 (the exponent bits), else through ldexp.
+__device__ __forceinline__ double pow2i(int e) {
+  return (e >= -1000 && e <= 1000) ? __longlong_as_double(static_cast<long long>(e + 1023) << 52) : ldexp(1.0, e);
 }
 
 // ------------------------------------------------------------------ int8 SYRK ----
@@ -274,7 +277,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     const long ra = 2 * a + row / 64;  // 64-row tile, the same for the warp's 32 lanes
     const int r = row % 64;
     const int* Ep = p.E + part * p.npad2;
-    const int er = Ep[a * 128 + row];
+    const double rs = pow2i(Ep[a * 128 + row]);  // row scale 2^e
     const uint32_t lane_base = tmem + (static_cast<uint32_t>(q * 32) << 16);
     bool ok = true;
     for (int pass = 0; pass < 2; ++pass) {
@@ -283,6 +286,9 @@ __global__ void __launch_bounds__(kI8Threads, 1)
         break;
       }
       tc_fence_after();
+      double gf[4];  // 2^-7(4 pass + g + 2)
+#pragma unroll
+      for (int g = 0; g < 4; ++g) gf[g] = pow2i(-7 * (4 * pass + g + 2));
 #pragma unroll 1
       for (int c0 = 0; c0 < 128; c0 += 16) {
         const long cb = 2 * b + c0 / 64;
@@ -300,9 +306,9 @@ __global__ void __launch_bounds__(kI8Threads, 1)
           for (int h = 0; h < 2; ++h) {
             double acc = 0.0;
 #pragma unroll
-            for (int g = 3; g >= 0; --g)  // smallest first
-              acc += ldexp(static_cast<double>(static_cast<int32_t>(v[g][j + h])), -7 * (4 * pass + g + 2));
-            w[h] = ldexp(acc, er + __ldg(Ep + b * 128 + c0 + j + h));
+            for (int g = 3; g >= 0; --g)  // smallest first; the group factors are exact powers of two
+              acc = fma(static_cast<double>(static_cast<int32_t>(v[g][j + h])), gf[g], acc);
+            w[h] = acc * (rs * pow2i(__ldg(Ep + b * 128 + c0 + j + h)));
           }
           double2* o = reinterpret_cast<double2*>(out + j);
           if (pass == 1) {
@@ -374,18 +380,18 @@ int sm_count(int device) {
 
 }  // namespace
 
-// Split-K parts of the int8 SYRK: chunk-aligned, at most kMaxPart k each, and enough CTAs for about
-// two waves (one CTA per SM), chosen among [want, 4 want] so that the last wave is fullest.
+// Split-K parts of the int8 SYRK: chunk-aligned, at most kMaxPart k each, and enough CTAs for
+// about two waves (one CTA per SM), chosen among [want, 4 want] so that the last wave is fullest.
 int syrk_i8_parts(long nt, long kdim, int device, long* kper_out) {
-  const long nb = (nt + 1) / 2, tiles = nb * (nb + 1) / 2;
+  const long nb = (nt + 1) / 2, ctas_per_part = nb * (nb + 1) / 2;
   const long sms = sm_count(device);
   const long nchunks = (kdim + kChunk - 1) / kChunk;
-  const long min_parts = (kdim + kMaxSlicePart - 1) / kMaxSlicePart;
-  const long want = std::max(min_parts, (2 * sms + tiles - 1) / tiles);
+  const long min_parts = (kdim + kMaxPart - 1) / kMaxPart;
+  const long want = std::max(min_parts, (2 * sms + ctas_per_part - 1) / ctas_per_part);
   long best = want;
   double best_eff = 0.0;
   for (long sp = want; sp <= 4 * want && sp <= std::max<long>(1, nchunks); ++sp) {
-    const long ctas = tiles * sp, waves = (ctas + sms - 1) / sms;
+    const long ctas = ctas_per_part * sp, waves = (ctas + sms - 1) / sms;
     const double eff = static_cast<double>(ctas) / static_cast<double>(waves * sms);
     if (eff > best_eff + 0.02) {
       best_eff = eff;
@@ -393,7 +399,7 @@ int syrk_i8_parts(long nt, long kdim, int device, long* kper_out) {
     }
   }
   long kper = round_up((kdim + best - 1) / best, kChunk);
-  kper = std::min(kper, kMaxSlicePart);
+  kper = std::min(kper, kMaxPart);
   *kper_out = kper;
   return static_cast<int>((kdim + kper - 1) / kper);
 }
@@ -412,25 +418,26 @@ int syrk_i8(rijk_ctx* ctx, const double* XT, long npad, long nt, long kdim, int 
   int* E = static_cast<int*>(ctx->Xe.p);
   k_slice_x<<<dim3(static_cast<unsigned>(npad2), static_cast<unsigned>(nparts)), kSliceThreads, 0, s>>>(
       XT, npad, npad2, kdim, kper, Xs, E);
-  CUtensorMap mX;
+  prof_mark(ctx, "slice_x");
+  CUtensorMap mA;
   const uint64_t cols = static_cast<uint64_t>(nblk) * kBlock;
-  if (!make_map_i8(&mX, Xs, cols, static_cast<uint64_t>(npad2), 128))
+  if (!make_map_i8(&mA, Xs, cols, static_cast<uint64_t>(npad2), 128))
     return set_err(ctx, RIJK_ERR_CUDA, "tensor map encoding failed (int8 digits)");
   I8Params ip{};
   ip.kdim = kdim;
   ip.kper = kper;
   ip.npad2 = static_cast<int>(npad2);
   ip.nt = static_cast<int>(nt);
-  ip.stages = std::min(4, static_cast<int>((kI8SmemBudget - 2048) / kI8Stage));
   ip.Kpart = Kpart;
   ip.ntile = nt * (nt + 1) / 2;
   ip.E = E;
   ip.err = static_cast<int*>(ctx->err.p);
+  ip.stages = std::min(4, static_cast<int>((kI8SmemBudget - 2048) / kI8Stage));
   const size_t smem = static_cast<size_t>(ip.stages) * kI8Stage + 1024 + 256;
   ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_i8), smem);
   const long nb = npad2 / 128;
   dim3 grid(static_cast<unsigned>(nb * (nb + 1) / 2), static_cast<unsigned>(nparts));
-  k_syrk_i8<<<grid, kI8Threads, smem, s>>>(mX, ip);
+  k_syrk_i8<<<grid, kI8Threads, smem, s>>>(mA, ip);
   return cuda_check(ctx, cudaGetLastError(), "int8 SYRK launch");
 }
 

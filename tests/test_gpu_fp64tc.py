@@ -41,10 +41,10 @@ def _check(V, I3, n, nocc, DM, MO):
 
 
 @pytest.mark.parametrize("n,naux,nocc", [(64, 40, 16), (150, 70, 1), (200, 96, 97), (333, 211, 45), (260, 48, 192),
-                                         (1000, 40, 48)])
+                                         (420, 60, 33), (580, 50, 40), (900, 36, 30), (1000, 40, 48)])
 def test_fp64tc_k_ragged_random(n, naux, nocc):
-    """naux * noccp = 70 * 16 ends in half a 32-wide chunk; n = 1000 fills 8 blocks of 128 rows, the last
-    one past npad."""
+    """naux * noccp = 70 * 16 ends in half a 32-wide chunk; n = 420, 580, 900 and 1000 end in a partly
+    filled block of 128 rows, and n = 1000 fills 8 such blocks, the last one past npad."""
     rng = np.random.default_rng(n + naux)
     A = rng.normal(size=(naux, naux))
     V = A @ A.T / naux + np.eye(naux)
