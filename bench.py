@@ -570,7 +570,8 @@ def main():
             r = r_best
             out[name] = {"seconds": el, "iterations": r["iterations"], "iterations_mixed": r["iterations_mixed"],
                          "energy": E, "ms_fock": r["ms_fock"], "ms_diag": r["ms_diag_phase"],
-                         "ms_inside": r["ms_total"],
+                         "ms_inside": r["ms_total"], "ms_setup": r["ms_setup_phase"],
+                         "ms_final": r["ms_final_phase"],
                          "converged": bool(r["converged"])}
             if name == "fp64":
                 E64 = E
@@ -582,7 +583,9 @@ def main():
                             "the switch")
         out["start"] = "superposition of atomic densities (%.2f s on the host, not in the SCF time)" % t_guess
         out["timing"] = ("wall time of rijk_scf, the fastest of three runs (ms_inside: the library's own clock of "
-                         "that run, without argument checks and buffer release)")
+                         "that run, without argument checks and buffer release; ms_setup: before the first "
+                         "iteration, uploads, overlap eigendecomposition and the guess's build and diagonalisation; "
+                         "ms_final: after the last iteration, closing build and orbitals)")
         scf = out
 
     cpu = {"skipped": cpu_skip} if cpu_skip else None

@@ -228,6 +228,10 @@ typedef struct {
   double history_energy[128];
   double history_diis_err[128];  /* per build: the DIIS error, or max |4 F_ai| in SOSCF steps      */
   int history_mixed[128]; /* 1 where the iteration used the mixed form                          */
+  double ms_setup_phase;  /* wall time before the first iteration: uploads, overlap
+                             eigendecomposition, the guess's Fock build and diagonalisation     */
+  double ms_final_phase;  /* wall time after the last iteration: the closing FP64 build (if any)
+                             and the orbitals' diagonalisation and download                     */
 } rijk_scf_result_t;
 
 /* Restricted Hartree-Fock on the GPU around the Fock build: the reference's RHF loop

@@ -217,19 +217,6 @@ __global__ void k_rot_build(const double* __restrict__ x, long nm, long nocc, do
   }
 }
 
-__global__ void k_copy_diag(const double* __restrict__ A, long nm, double* __restrict__ d) {
-  for (long i = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; i < nm;
-       i += static_cast<long>(gridDim.x) * blockDim.x)
-    d[i] = A[i * (nm + 1)];
-}
-
-// column j of Q (column-major nm x nm) times sign(d[j]): the QR factor with R's diagonal positive
-__global__ void k_sign_cols(double* __restrict__ Q, long nm, const double* __restrict__ d) {
-  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < nm * nm;
-       idx += static_cast<long>(gridDim.x) * blockDim.x)
-    if (d[idx / nm] < 0.0) Q[idx] = -Q[idx];
-}
-
 unsigned grid_of(long total) {
   long b = (total + 255) / 256;
   if (b > 148L * 8) b = 148L * 8;
@@ -480,6 +467,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     if (diag(pH, soscf || hybrid) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the core Hamiltonian failed");
   }
   density(pD);
+  const auto t_loop0 = std::chrono::steady_clock::now();
 
   int prec = o.precision;
   int nmix = 0, nbuild = 0, m = 0, head = 0;
@@ -632,8 +620,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
                                          : static_cast<int>(std::min<long>(nm, std::min(20, o.max_iter)));
     const size_t nmm = static_cast<size_t>(nm) * nm;
     DeviceBuf lb, qrw;
-    int lw_qr = 0, lw_or = 0;
-    if ((rc = ensure(ctx, lb, ((2 * static_cast<size_t>(mvec) + 8) * dimc + 2 * nmm + 2 * nm) * sizeof(double),
+    int lw_chol = 0;
+    if ((rc = ensure(ctx, lb, ((2 * static_cast<size_t>(mvec) + 8) * dimc + 2 * nmm) * sizeof(double),
                      "scf L-BFGS"))) {
       cleanup();
       return rc;
@@ -647,17 +635,14 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     double* ysc = gprev + dimc;               // g - gprev
     double* Yv = ysc + dimc;                  // mvec gradient differences
     double* Sv = Yv + mvec * dimc;            // mvec steps, slot mvec = the last step taken
-    double* Fmo = Sv + (mvec + 1) * dimc;     // C^T F C
-    double* Rq = Fmo + nmm;                   // rotation, then its orthonormal rows
-    double* tau = Rq + nmm;
-    double* rdg = tau + nm;
+    double* Fmo = Sv + (mvec + 1) * dimc;     // C^T F C, then the Gram matrix of the rotation
+    double* Rq = Fmo + nmm;                   // rotation, then its orthonormal columns
     cudaMemsetAsync(lb.p, 0, lb.bytes, s);
-    if (cusolverDnDgeqrf_bufferSize(cs, nmi, nmi, Rq, nmi, &lw_qr) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnDorgqr_bufferSize(cs, nmi, nmi, nmi, Rq, nmi, tau, &lw_or) != CUSOLVER_STATUS_SUCCESS) {
+    if (cusolverDnDpotrf_bufferSize(cs, CUBLAS_FILL_MODE_UPPER, nmi, Fmo, nmi, &lw_chol) != CUSOLVER_STATUS_SUCCESS) {
       release(lb);
-      return fail(RIJK_ERR_SOLVER, "QR buffer query failed");
+      return fail(RIJK_ERR_SOLVER, "Cholesky buffer query failed");
     }
-    const int lwq = std::max(std::max(lw_qr, lw_or), 1);
+    const int lwq = std::max(lw_chol, 1);
     if ((rc = ensure(ctx, qrw, static_cast<size_t>(lwq) * sizeof(double), "scf QR work"))) {
       release(lb);
       cleanup();
@@ -775,14 +760,19 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       ++step_num;
       auto td = now();
       t_diis += msec(tc, td);
-      // orbitals <- (orthonormalised I + X - X^T) orbitals (src/converger_2_1.cpp:105-123)
+      // orbitals <- (orthonormalised I + X - X^T) orbitals (src/converger_2_1.cpp:105-123).  The
+      // reference orthonormalises the columns in order (Gram-Schmidt): A = Q R with R's diagonal
+      // positive, a unique factorisation.  Here Q comes from two Cholesky-QR passes, A^T A = U^T U and
+      // A <- A U^-1: A = I + X - X^T has singular values in [1, sqrt(1 + |X|^2)], so A^T A is well
+      // conditioned, and the second pass brings Q^T Q to I within rounding.
       k_rot_build<<<grid_of(nm * nm), 256, 0, s>>>(xs, nm, nocc, Rq);
-      if (cusolverDnDgeqrf(cs, nmi, nmi, Rq, nmi, tau, pQw, lwq, pInfo) != CUSOLVER_STATUS_SUCCESS)
-        return fail2(RIJK_ERR_SOLVER, "geqrf of the rotation failed");
-      k_copy_diag<<<grid_of(nm), 256, 0, s>>>(Rq, nm, rdg);
-      if (cusolverDnDorgqr(cs, nmi, nmi, nmi, Rq, nmi, tau, pQw, lwq, pInfo) != CUSOLVER_STATUS_SUCCESS)
-        return fail2(RIJK_ERR_SOLVER, "orgqr of the rotation failed");
-      k_sign_cols<<<grid_of(nm * nm), 256, 0, s>>>(Rq, nm, rdg);
+      for (int pass = 0; pass < 2; ++pass) {
+        cublasDsyrk(cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nmi, nmi, &one, Rq, nmi, &zero, Fmo, nmi);  // A^T A
+        if (cusolverDnDpotrf(cs, CUBLAS_FILL_MODE_UPPER, nmi, Fmo, nmi, pQw, lwq, pInfo) != CUSOLVER_STATUS_SUCCESS)
+          return fail2(RIJK_ERR_SOLVER, "Cholesky factorisation of the rotation's Gram matrix failed");
+        cublasDtrsm(cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nmi, nmi, &one,
+                    Fmo, nmi, Rq, nmi);  // A U^-1
+      }
       cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, nmi, &one, pC, ni, Rq, nmi, &zero, pT1, ni);  // C Q
       cudaMemcpyAsync(pC, pT1, static_cast<size_t>(n) * nm * sizeof(double), cudaMemcpyDeviceToDevice, s);
       density(pDn);
@@ -795,6 +785,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     release(lb);
     release(qrw);
   }
+  const auto t_loop1 = std::chrono::steady_clock::now();
   // The energy is the last FP64 build's, as the reference reports it (src/SCF.cpp:134-156): a run
   // that ended in the mixed phase gets one FP64 build at its density for it.
   if (last_prec == RIJK_PREC_MIXED || last_prec < 0) {
@@ -833,8 +824,10 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   result->ms_build_phase = t_build;
   result->ms_diis_phase = t_diis;
   result->ms_diag_phase = t_diag;
-  result->ms_total =
-      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  const auto t_end = std::chrono::steady_clock::now();
+  result->ms_total = std::chrono::duration<double, std::milli>(t_end - t_start).count();
+  result->ms_setup_phase = std::chrono::duration<double, std::milli>(t_loop0 - t_start).count();
+  result->ms_final_phase = std::chrono::duration<double, std::milli>(t_end - t_loop1).count();
   cleanup();
   if (!converged) return set_err(ctx, RIJK_ERR_CONVERGE, "rijk_scf: not converged in %d iterations", o.max_iter);
   return RIJK_OK;

@@ -74,7 +74,8 @@ class ScfResult(ctypes.Structure):
                 ("ms_build_phase", ctypes.c_double), ("ms_diis_phase", ctypes.c_double),
                 ("ms_diag_phase", ctypes.c_double), ("history_len", ctypes.c_int),
                 ("history_energy", ctypes.c_double * 128), ("history_diis_err", ctypes.c_double * 128),
-                ("history_mixed", ctypes.c_int * 128)]
+                ("history_mixed", ctypes.c_int * 128), ("ms_setup_phase", ctypes.c_double),
+                ("ms_final_phase", ctypes.c_double)]
 
 
 class RijkError(RuntimeError):
