@@ -571,7 +571,7 @@ def main():
             out[name] = {"seconds": el, "iterations": r["iterations"], "iterations_mixed": r["iterations_mixed"],
                          "energy": E, "ms_fock": r["ms_fock"], "ms_diag": r["ms_diag_phase"],
                          "ms_inside": r["ms_total"], "ms_setup": r["ms_setup_phase"],
-                         "ms_final": r["ms_final_phase"],
+                         "ms_final": r["ms_final_phase"], "purified": r["purified"],
                          "converged": bool(r["converged"])}
             if name == "fp64":
                 E64 = E

@@ -203,6 +203,12 @@ typedef struct {
   double conv_grad;       /* SOSCF: converged when max |4 F_ai| < conv_grad; default 1e-7          */
   double conv_energy;     /* SOSCF: or when |E - E_previous| < conv_energy; default 1e-10          */
   int lbfgs_vectors;      /* SOSCF: curvature pairs kept, 1 .. 32; default min(n_mo, 20, max_iter)  */
+  int density_by_eigenvectors; /* DIIS: 0 (default) takes each new density's occupied space from
+                             trace-correcting purification of X^T F X (products only) and one
+                             subspace step from the previous orbitals, falling back to the
+                             eigensolver when either does not converge; 1 diagonalises every
+                             step, as the reference (src/SCF.cpp:160-166).  Same densities to
+                             rounding                                                        */
 } rijk_scf_opts_t;
 
 #define RIJK_CONV_DIIS 0
@@ -232,6 +238,7 @@ typedef struct {
                              eigendecomposition, the guess's Fock build and diagonalisation     */
   double ms_final_phase;  /* wall time after the last iteration: the closing FP64 build (if any)
                              and the orbitals' diagonalisation and download                     */
+  int purified;           /* DIIS steps whose occupied orbitals came from purification          */
 } rijk_scf_result_t;
 
 /* Restricted Hartree-Fock on the GPU around the Fock build: the reference's RHF loop

@@ -223,6 +223,118 @@ unsigned grid_of(long total) {
   return static_cast<unsigned>(b < 1 ? 1 : b);
 }
 
+// ---- occupied projector by trace-correcting purification (TC2: A. M. N. Niklasson, Phys. Rev. B 66,
+// 155115 (2002)).  The new density of a DIIS step is the projector on the n_c lowest eigenvectors of
+// F' = X^T F X; purification reaches it with n' x n' products alone.  F' is mapped to
+// P0 = (b I - F') / 2b, b = max_j sum_i |F'_ij| >= its spectral radius, so P0's eigenvalues lie in
+// [0, 1] with the occupied ones highest; each step P <- P^2 or 2P - P^2, whichever trace is nearer
+// n_c, drives them to 1 and the rest to 0 while keeping the eigenvectors.
+
+// out[j] = sum_i |A_ij| (column-major n x n; for a symmetric A the absolute row sums): a warp per column
+__global__ void k_col_abs_sum(const double* __restrict__ A, long n, double* __restrict__ out) {
+  const long j = static_cast<long>(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const int lane = threadIdx.x & 31;
+  double acc = 0.0;
+  for (long i = lane; i < n; i += 32) acc += fabs(A[i + j * n]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[j] = acc;
+}
+
+// One block: sc[slot] = the largest of v[0 .. n) (1 if that is 0).
+__global__ void k_max_small(const double* __restrict__ v, long n, double* __restrict__ sc, int slot) {
+  __shared__ double sh[32];
+  double m = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, v[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < static_cast<int>(blockDim.x / 32); ++w) m = fmax(m, sh[w]);
+    m = fmax(m, sh[0]);
+    sc[slot] = m > 0.0 ? m : 1.0;
+  }
+}
+
+// A <- (b I - A) / 2b in place, b = sc[0]
+__global__ void k_purify_init(double* __restrict__ A, long n, const double* __restrict__ sc) {
+  const double b = sc[0], h = 0.5 / b;
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < n * n;
+       idx += static_cast<long>(gridDim.x) * blockDim.x)
+    A[idx] = ((idx % n == idx / n ? b : 0.0) - A[idx]) * h;
+}
+
+// One block: sc[1] = tr P, sc[2] = tr P2 (a fixed summation order)
+__global__ void k_tc2_traces(const double* __restrict__ P, const double* __restrict__ P2, long n,
+                             double* __restrict__ sc) {
+  __shared__ double sh[2][32];
+  double a = 0.0, c = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) {
+    a += P[i * (n + 1)];
+    c += P2[i * (n + 1)];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = a;
+    sh[1][threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = 0.0;
+    c = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w) {
+      a += sh[0][w];
+      c += sh[1][w];
+    }
+    sc[1] = a;
+    sc[2] = c;
+  }
+}
+
+// P <- P2 when tr P2 is nearer n_c than tr(2P - P2), else 2P - P2 (traces from sc)
+__global__ void k_tc2_update(double* __restrict__ P, const double* __restrict__ P2, long total,
+                             const double* __restrict__ sc, double nocc) {
+  const double t1 = sc[1], t2 = sc[2];
+  const bool square = fabs(t2 - nocc) < fabs(2.0 * t1 - t2 - nocc);
+  for (long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<long>(gridDim.x) * blockDim.x)
+    P[idx] = square ? P2[idx] : 2.0 * P[idx] - P2[idx];
+}
+
+// One block: sc[slot] = min_i |R_ii| / max_i |R_ii| of a Cholesky factor (n x n, column-major)
+__global__ void k_chol_ratio(const double* __restrict__ R, long n, double* __restrict__ sc, int slot) {
+  __shared__ double sh[2][32];
+  double lo = 1e300, hi = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) {
+    const double d = fabs(R[i * (n + 1)]);
+    lo = fmin(lo, d);
+    hi = fmax(hi, d);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = lo;
+    sh[1][threadIdx.x >> 5] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w) {
+      lo = fmin(lo, sh[0][w]);
+      hi = fmax(hi, sh[1][w]);
+    }
+    sc[slot] = hi > 0.0 && lo == lo ? lo / hi : 0.0;
+  }
+}
+
 // Solves the (m+1) x (m+1) Pulay system by Gaussian elimination with partial pivoting.
 bool diis_coefficients(const std::vector<double>& Bm, int m, std::vector<double>& c) {
   const int N = m + 1;
@@ -301,9 +413,10 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   constexpr long kMixedRows = 192;  // orbitals one mixed build takes
 
   DeviceBuf dH, dS, dX, dF, dFex, dD, dDn, dC, dJ, dK, dT1, dT2, dE, dW, dU, work, info, red, out, ring_F, ring_E;
+  DeviceBuf dV, dPur, dInfo2;  // occupied eigenvectors (X basis), purification scalars, Cholesky infos
   auto cleanup = [&]() {
-    DeviceBuf* all[] = {&dH, &dS, &dX, &dF, &dFex, &dD, &dDn, &dC, &dJ, &dK, &dT1, &dT2,
-                        &dE, &dW, &dU, &work, &info, &red, &out, &ring_F, &ring_E};
+    DeviceBuf* all[] = {&dH, &dS, &dX, &dF, &dFex, &dD, &dDn, &dC, &dJ, &dK, &dT1, &dT2, &dE, &dW, &dU,
+                        &work, &info, &red, &out, &ring_F, &ring_E, &dV, &dPur, &dInfo2};
     for (DeviceBuf* b : all) release(*b);
   };
   const size_t b_nn = nn * sizeof(double);
@@ -318,7 +431,10 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       (rc = ensure(ctx, red, 2 * kRedBlocks * sizeof(double), "scf reduce")) ||
       (rc = ensure(ctx, out, kOutSlots * sizeof(double), "scf out")) ||
       (rc = ensure(ctx, ring_F, static_cast<size_t>(m_max) * b_nn, "scf DIIS F")) ||
-      (rc = ensure(ctx, ring_E, static_cast<size_t>(m_max) * b_nn, "scf DIIS e"))) {
+      (rc = ensure(ctx, ring_E, static_cast<size_t>(m_max) * b_nn, "scf DIIS e")) ||
+      (rc = ensure(ctx, dV, static_cast<size_t>(n) * std::max<long>(nocc, 1) * sizeof(double), "scf V")) ||
+      (rc = ensure(ctx, dPur, 16 * sizeof(double), "scf purification")) ||
+      (rc = ensure(ctx, dInfo2, 4 * sizeof(int), "scf Cholesky info"))) {
     cleanup();
     return rc;
   }
@@ -340,6 +456,9 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   double* pOut = static_cast<double*>(out.p);
   double* rF = static_cast<double*>(ring_F.p);
   double* rE = static_cast<double*>(ring_E.p);
+  double* pV = static_cast<double*>(dV.p);
+  double* pPur = static_cast<double*>(dPur.p);
+  int* pInfo2 = static_cast<int*>(dInfo2.p);
   int* pInfo = static_cast<int*>(info.p);
   const double one = 1.0, zero = 0.0;
 
@@ -397,8 +516,13 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   if (cusolverDnDsyevdx_bufferSize(cs, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER, nmi,
                                    pU, nmi, 0.0, 0.0, 1, nev, &meig, pW, &lworkx) != CUSOLVER_STATUS_SUCCESS)
     return fail(RIJK_ERR_SOLVER, "syevdx buffer query failed");
-  if (lworkx > lwork) {
-    if ((rc = ensure(ctx, work, static_cast<size_t>(lworkx) * sizeof(double), "scf syevdx work"))) {
+  int lworkp = 0;  // Cholesky of the n_c x n_c Gram matrix in the purification step
+  if (nocc > 0 && cusolverDnDpotrf_bufferSize(cs, CUBLAS_FILL_MODE_UPPER, static_cast<int>(nocc), pT2,
+                                              static_cast<int>(nocc), &lworkp) != CUSOLVER_STATUS_SUCCESS)
+    return fail(RIJK_ERR_SOLVER, "Cholesky buffer query failed");
+  if (std::max(lworkx, lworkp) > lwork) {
+    if ((rc = ensure(ctx, work, static_cast<size_t>(std::max(lworkx, lworkp)) * sizeof(double),
+                     "scf syevdx work"))) {
       cleanup();
       return rc;
     }
@@ -421,7 +545,66 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       ncols = nev;
     }
     cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, ncols, nmi, &one, pX, ni, pU, nmi, &zero, pC, ni);  // C = X V
+    if (nocc > 0)  // the occupied eigenvectors start the next purification step's subspace
+      cudaMemcpyAsync(pV, pU, static_cast<size_t>(nm) * nocc * sizeof(double), cudaMemcpyDeviceToDevice, s);
     return RIJK_OK;
+  };
+  // The occupied orbitals of a DIIS step without an eigensolver: the projector P on the n_c lowest
+  // eigenvectors of F' = X^T F X by TC2 purification, then C = X Q with Q an orthonormal basis of
+  // P V (V the previous step's occupied orbitals) from two Cholesky-QR passes.  D = C C^T and K
+  // depend on C only through that projector, so the step is the eigenvector step's to rounding.
+  // Returns 0, 1 when the caller should use the eigensolver (no convergence, a subspace too far
+  // from the previous one), or an error code.
+  int purified = 0;
+  auto purify_occ = [&](const double* Fm) -> int {
+    constexpr int kMaxSteps = 100;
+    if (o.density_by_eigenvectors || nocc <= 0 || nocc >= nm) return 1;
+    const int no = static_cast<int>(nocc);
+    double sc[8];
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nmi, ni, &one, Fm, ni, pX, ni, &zero, pT1, ni);    // F X
+    cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nmi, nmi, ni, &one, pX, ni, pT1, ni, &zero, pU, nmi);  // X^T F X
+    double* P = pU;
+    double* P2 = pT2;
+    k_col_abs_sum<<<static_cast<unsigned>((nm + 7) / 8), 256, 0, s>>>(P, nm, pW);
+    k_max_small<<<1, 256, 0, s>>>(pW, nm, pPur, 0);
+    k_purify_init<<<grid_of(nm * nm), 256, 0, s>>>(P, nm, pPur);
+    int left = -1;  // steps still to take once the idempotency error is small
+    bool done = false;
+    for (int step = 1; step <= kMaxSteps && !done; ++step) {
+      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, nmi, nmi, nmi, &one, P, nmi, P, nmi, &zero, P2, nmi);  // P^2
+      k_tc2_traces<<<1, 256, 0, s>>>(P, P2, nm, pPur);
+      k_tc2_update<<<grid_of(nm * nm), 256, 0, s>>>(P, P2, nm * nm, pPur, static_cast<double>(nocc));
+      if (left > 0) {
+        done = --left == 0;
+      } else if (step >= 16 && step % 4 == 0) {
+        // tr P - tr P^2 = sum lambda (1 - lambda) over P's eigenvalues, before this step
+        cudaMemcpyAsync(sc, pPur, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return RIJK_ERR_CUDA;
+        if (std::fabs(sc[1] - sc[2]) < 1e-8) left = 2;  // quadratic from here: two steps reach rounding
+      }
+    }
+    if (!done) return 1;
+    // W = P V, orthonormalised: W^T W = U^T U, W <- W U^-1, twice
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, nmi, no, nmi, &one, P, nmi, pV, nmi, &zero, pT1, nmi);
+    for (int pass = 0; pass < 2; ++pass) {
+      cublasDsyrk(cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, no, nmi, &one, pT1, nmi, &zero, P2, no);
+      if (cusolverDnDpotrf(cs, CUBLAS_FILL_MODE_UPPER, no, P2, no, pWork, std::max(lworkp, 1), pInfo2 + pass) !=
+          CUSOLVER_STATUS_SUCCESS)
+        return 1;
+      if (pass == 0) k_chol_ratio<<<1, 256, 0, s>>>(P2, no, pPur, 4);
+      cublasDtrsm(cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nmi, no, &one, P2,
+                  no, pT1, nmi);
+    }
+    int hinfo2[2] = {1, 1};
+    cudaMemcpyAsync(sc, pPur, 5 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hinfo2, pInfo2, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return RIJK_ERR_CUDA;
+    // the last step's trace is n_c; the subspace step kept its rank (cond(P V) below 1e6)
+    if (hinfo2[0] != 0 || hinfo2[1] != 0 || !(sc[4] > 1e-6) || !(std::fabs(sc[1] - nocc) < 1e-6)) return 1;
+    cudaMemcpyAsync(pV, pT1, static_cast<size_t>(nm) * no * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, no, nmi, &one, pX, ni, pT1, nmi, &zero, pC, ni);  // C = X Q
+    ++purified;
+    return 0;
   };
   auto density = [&](double* Dm) {  // D = C_occ C_occ^T
     if (nocc > 0)
@@ -595,7 +778,9 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       }
       auto tc = now();
       t_diis += msec(tb, tc);
-      if (diag(pFex) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
+      const int pr = purify_occ(pFex);
+      if (pr > 1) return fail(pr, "purification of the Fock matrix failed");
+      if (pr == 1 && diag(pFex) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
       have_fex = true;
       density(pDn);
       reduce(DiffSqF{pDn, pD}, nn, 0, 0);
@@ -828,6 +1013,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   result->ms_total = std::chrono::duration<double, std::milli>(t_end - t_start).count();
   result->ms_setup_phase = std::chrono::duration<double, std::milli>(t_loop0 - t_start).count();
   result->ms_final_phase = std::chrono::duration<double, std::milli>(t_end - t_loop1).count();
+  result->purified = purified;
   cleanup();
   if (!converged) return set_err(ctx, RIJK_ERR_CONVERGE, "rijk_scf: not converged in %d iterations", o.max_iter);
   return RIJK_OK;

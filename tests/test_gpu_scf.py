@@ -144,3 +144,29 @@ def test_gpu_scf_diis_then_soscf(start):
     assert h[-1][1] < 1e-7 or abs(h[-1][0] - h[-2][0]) < 1e-10
     C = MO[:rh["nmo"]]
     assert np.max(np.abs(C @ si.S @ C.T - np.eye(rh["nmo"]))) < 1e-9
+
+
+@pytest.mark.parametrize("precision", [rijk.PREC_FP64, rijk.PREC_MIXED])
+def test_gpu_scf_purified_densities_match_eigenvectors(precision):
+    """DIIS densities from TC2 purification of X^T F X (the default) against the eigenvector step of
+    the reference: the same iterates to rounding, so the same build count and energy to 1e-10 Eh.
+    With FP64 builds the per-iteration energies and DIIS errors agree to 1e-9.  A split-BF16 build
+    moves by up to its own rounding (about 1e-5 Eh here, against an error of about 1e-3 Eh per
+    build) when D changes by one rounding, and the FP64 phase starts from where the mixed one
+    ended, so the mixed run is held to its final energy and build counts."""
+    si = ints.SystemIntegrals(water_cluster((2, 3), seed=3), "cc-pvdz", "cc-pvdz-jkfit")
+    guess = si.sad()
+    with rijk.FockBuilder(0) as fb:
+        fb.set_metric(si.V)
+        fb.set_3c(si.I3, si.n)
+        Ee, _, re_ = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess, precision=precision, purify=False)
+        Ep, MO, rp = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess, precision=precision)
+    assert re_["converged"] and rp["converged"]
+    assert re_["purified"] == 0 and rp["purified"] > 0
+    assert rp["iterations"] == re_["iterations"] and rp["iterations_mixed"] == re_["iterations_mixed"]
+    assert abs(Ep - Ee) < 1e-10, (Ep, Ee)
+    if precision == rijk.PREC_FP64:
+        for (a, b, _), (c, d, _) in zip(rp["history"], re_["history"]):
+            assert abs(a - c) < 1e-9 and abs(b - d) < 1e-9 * max(1.0, abs(d)), (a, c, b, d)
+    C = MO[:rp["nmo"]]
+    assert np.max(np.abs(C @ si.S @ C.T - np.eye(rp["nmo"]))) < 1e-9
