@@ -82,20 +82,39 @@ __global__ void k_reduce_max_partial(F f, long n, double* __restrict__ partial) 
 }
 
 // out[slot] = sum (compensated, partials and their compensations) or max of the kRedBlocks
-// partials, in a fixed order.
+// partials, in a fixed order: launched with kRedBlocks threads, thread b takes partial b, then a
+// fixed shuffle tree per warp and the warps in order (deterministic).
 __global__ void k_reduce_final(const double* __restrict__ partial, int is_max, double* __restrict__ out, int slot) {
-  if (threadIdx.x != 0) return;
+  __shared__ double sh[2][kRedBlocks / 32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if (is_max) {
-    double m = 0.0;
-    for (int b = 0; b < kRedBlocks; ++b) m = fmax(m, partial[b]);
-    out[slot] = m;
-  } else {
-    double s = 0.0, c = 0.0;
-    for (int b = 0; b < kRedBlocks; ++b) {
-      neumaier_add(s, c, partial[b]);
-      c += partial[kRedBlocks + b];
+    double m = partial[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) sh[0][warp] = m;
+    __syncthreads();
+    if (t == 0) {
+      m = sh[0][0];
+      for (int w = 1; w < kRedBlocks / 32; ++w) m = fmax(m, sh[0][w]);
+      out[slot] = m;
     }
-    out[slot] = s + c;
+  } else {
+    double v = partial[t], c = partial[kRedBlocks + t];
+    warp_sum_comp(v, c);
+    if (lane == 0) {
+      sh[0][warp] = v;
+      sh[1][warp] = c;
+    }
+    __syncthreads();
+    if (t == 0) {
+      v = sh[0][0];
+      c = sh[1][0];
+      for (int w = 1; w < kRedBlocks / 32; ++w) {
+        neumaier_add(v, c, sh[0][w]);
+        c += sh[1][w];
+      }
+      out[slot] = v + c;
+    }
   }
 }
 
@@ -678,6 +697,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   auto msec = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
   if (!soscf) {
     bool have_fex = false;  // pFex holds the matrix whose eigenvectors gave pD
+    std::vector<double> Bcache(32 * 32, 0.0);  // Pulay matrix entries by ring slot
     for (int it = 0; it < o.max_iter; ++it) {
       auto ta = now();
       if ((rc = build(prec))) {
@@ -751,23 +771,26 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       }
       m = m < m_max ? m + 1 : m_max;
       head = (head + 1) % m_max;
-      // Pulay B matrix over the stored error vectors
+      // Pulay B matrix over the stored error vectors.  Only the newest vector's row is new: the
+      // other entries were formed when the later vector of each pair was stored, and are kept per
+      // ring slot (each pair's dot product is formed once, by the same reduction).
       std::vector<double> Bm(static_cast<size_t>(m) * m);
       {
         int slots[32];
         for (int i = 0; i < m; ++i) slots[i] = (head - m + i + m_max) % m_max;
+        const int knew = slots[m - 1];
         for (int i = 0; i < m; ++i)
-          for (int j = 0; j <= i; ++j)
-            reduce(DotF{rE + static_cast<size_t>(slots[i]) * nn, rE + static_cast<size_t>(slots[j]) * nn}, nm * nm, 0,
-                   2 + i * (i + 1) / 2 + j);
-        std::vector<double> tmp(kOutSlots);
-        cudaMemcpyAsync(tmp.data(), pOut, kOutSlots * sizeof(double), cudaMemcpyDeviceToHost, s);
+          reduce(DotF{rE + static_cast<size_t>(knew) * nn, rE + static_cast<size_t>(slots[i]) * nn}, nm * nm, 0,
+                 2 + i);
+        std::vector<double> tmp(2 + m);
+        cudaMemcpyAsync(tmp.data(), pOut, (2 + m) * sizeof(double), cudaMemcpyDeviceToHost, s);
         if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf DIIS"))) {
           cleanup();
           return rc;
         }
+        for (int i = 0; i < m; ++i) Bcache[knew * 32 + slots[i]] = Bcache[slots[i] * 32 + knew] = tmp[2 + i];
         for (int i = 0; i < m; ++i)
-          for (int j = 0; j <= i; ++j) Bm[i * m + j] = Bm[j * m + i] = tmp[2 + i * (i + 1) / 2 + j];
+          for (int j = 0; j < m; ++j) Bm[i * m + j] = Bcache[slots[i] * 32 + slots[j]];
         std::vector<double> c;
         if (!diis_coefficients(Bm, m, c)) {
           c.assign(m, 0.0);
