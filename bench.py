@@ -556,14 +556,17 @@ def main():
         runs = (("fp64", rijk.PREC_FP64, rijk.CONV_DIIS), ("mixed_then_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS),
                 ("soscf_fp64", rijk.PREC_FP64, rijk.CONV_SOSCF),
                 ("soscf_mixed_then_fp64", rijk.PREC_MIXED, rijk.CONV_SOSCF),
-                ("diis_mixed_then_soscf_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF))
+                ("diis_mixed_then_soscf_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF),
+                ("diis_mixed_then_soscf_fp64tc", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF))
         for name, prec, conv in runs:
+            # the last variant's FP64-accurate phase uses FP64_TC builds (K on the int8 tensor cores)
+            fp64_phase = rijk.PREC_FP64_TC if name.endswith("fp64tc") else rijk.PREC_FP64
             el = None
             for _ in range(3):  # the fastest of three runs: host-side latencies make single SCF timings noisy
                 torch.cuda.synchronize(dev)
                 t0 = time.perf_counter()
                 E, _, r = fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, conv_dm_rms=1e-10, guess=guess,
-                                 converger=conv)
+                                 converger=conv, fp64_phase=fp64_phase)
                 t = time.perf_counter() - t0
                 if el is None or t < el:
                     el, r_best = t, r

@@ -209,6 +209,9 @@ typedef struct {
                              eigensolver when either does not converge; 1 diagonalises every
                              step, as the reference (src/SCF.cpp:160-166).  Same densities to
                              rounding                                                        */
+  int fp64_phase_precision; /* 0 (default): RIJK_PREC_FP64 builds after a mixed phase (and for a
+                             closing build); RIJK_PREC_FP64_TC: the same FP64-accurate results
+                             with K on the int8 tensor cores                                    */
 } rijk_scf_opts_t;
 
 #define RIJK_CONV_DIIS 0

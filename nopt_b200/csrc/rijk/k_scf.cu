@@ -416,6 +416,10 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   const bool hybrid = o.converger == RIJK_CONV_DIIS_SOSCF;   // DIIS, then SOSCF from the switch on
   int rc = check_fock_args(ctx, nocc, o.precision);
   if (rc) return rc;
+  if (o.fp64_phase_precision != 0 && o.fp64_phase_precision != RIJK_PREC_FP64_TC)
+    return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: fp64_phase_precision must be 0 (FP64) or RIJK_PREC_FP64_TC");
+  // the form of the FP64-accurate builds after a mixed phase, and of a closing build
+  const int prec_fp64 = o.fp64_phase_precision == RIJK_PREC_FP64_TC ? RIJK_PREC_FP64_TC : RIJK_PREC_FP64;
   if (o.diis_size > 32) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: diis_size above 32");
   if (o.guess_dm && (!o.guess_rows || o.guess_nrows <= 0 || o.guess_nrows > round_up(ctx->n, 16)))
     return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: guess needs factor rows (1 .. n_ao of them)");
@@ -744,7 +748,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
         stalled = since_best >= 5 || nmix >= o.max_iter / 2;
       }
       if (prec == RIJK_PREC_MIXED && (err < o.switch_diis_err || stalled)) {
-        prec = RIJK_PREC_FP64;
+        prec = prec_fp64;
         if (hybrid) {
           // to the SOSCF loop, which rebuilds F in FP64 for this density.  It needs every
           // orbital: those of the extrapolated matrix this density came from (or, before the
@@ -916,7 +920,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
         }
         if (err < o.switch_diis_err || since_best >= 5 || nmix >= o.max_iter / 2) {
           // to the FP64 form: rebuild F for the same orbitals, restart the L-BFGS history
-          prec = RIJK_PREC_FP64;
+          prec = prec_fp64;
           step_num = 0;
           E_old = 1e15;
           --it;
@@ -997,7 +1001,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   // The energy is the last FP64 build's, as the reference reports it (src/SCF.cpp:134-156): a run
   // that ended in the mixed phase gets one FP64 build at its density for it.
   if (last_prec == RIJK_PREC_MIXED || last_prec < 0) {
-    if ((rc = build(RIJK_PREC_FP64))) {
+    if ((rc = build(prec_fp64))) {
       cleanup();
       return rc;
     }

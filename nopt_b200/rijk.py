@@ -64,7 +64,8 @@ class ScfOpts(ctypes.Structure):
                 ("diis_keep_on_switch", ctypes.c_int), ("lindep", ctypes.c_double),
                 ("guess_dm", _dp), ("guess_rows", _dp), ("guess_nrows", ctypes.c_long),
                 ("converger", ctypes.c_int), ("conv_grad", ctypes.c_double), ("conv_energy", ctypes.c_double),
-                ("lbfgs_vectors", ctypes.c_int), ("density_by_eigenvectors", ctypes.c_int)]
+                ("lbfgs_vectors", ctypes.c_int), ("density_by_eigenvectors", ctypes.c_int),
+                ("fp64_phase_precision", ctypes.c_int)]
 
 
 class ScfResult(ctypes.Structure):
@@ -278,19 +279,21 @@ class FockBuilder:
 
     def scf(self, H, S, n_c, e_nuc, precision=PREC_FP64, conv_dm_rms=1e-10, switch_diis_err=1e-5, max_iter=100,
             diis_size=8, guess=None, diis_keep_on_switch=False, converger=CONV_DIIS, conv_grad=1e-7,
-            conv_energy=1e-10, lbfgs_vectors=0, purify=True):
+            conv_energy=1e-10, lbfgs_vectors=0, purify=True, fp64_phase=PREC_FP64):
         """RHF on the GPU (rijk_scf); guess = (D0, R) with D0 = R^T R (e.g. SystemIntegrals.sad()),
         None for the core-Hamiltonian start; converger CONV_DIIS, CONV_SOSCF (the reference's
         L-BFGS orbital rotations, converged on max|4 F_ai| < conv_grad or |dE| < conv_energy), or
         CONV_DIIS_SOSCF (DIIS while the builds are mixed, SOSCF from the switch to FP64 on).
         purify=False diagonalises X^T F X at every DIIS step (the reference's step); the default
         takes the occupied space from purification, with the eigensolver as its fallback.
+        fp64_phase=PREC_FP64_TC makes the builds after a mixed phase FP64_TC ones.
         Returns (E, MO rows, result dict)."""
         n = self.n
         o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1 if diis_keep_on_switch else 0,
                     1e-10)
         o.converger, o.conv_grad, o.conv_energy, o.lbfgs_vectors = converger, conv_grad, conv_energy, lbfgs_vectors
         o.density_by_eigenvectors = 0 if purify else 1
+        o.fp64_phase_precision = 0 if fp64_phase == PREC_FP64 else fp64_phase
         if guess is not None:
             gD, gR = _c(guess[0]), _c(guess[1])
             o.guess_dm, o.guess_rows, o.guess_nrows = _p(gD), _p(gR), gR.shape[0]

@@ -170,3 +170,21 @@ def test_gpu_scf_purified_densities_match_eigenvectors(precision):
             assert abs(a - c) < 1e-9 and abs(b - d) < 1e-9 * max(1.0, abs(d)), (a, c, b, d)
     C = MO[:rp["nmo"]]
     assert np.max(np.abs(C @ si.S @ C.T - np.eye(rp["nmo"]))) < 1e-9
+
+
+def test_gpu_scf_fp64_phase_on_int8_tensor_cores():
+    """fp64_phase=PREC_FP64_TC: after the mixed phase the builds are FP64_TC ones (K from exact int8
+    digit products), FP64-accurate, so the run ends on the FP64 energy; other values are refused."""
+    si = ints.SystemIntegrals(water_cluster((2, 3), seed=4), "cc-pvdz", "cc-pvdz-jkfit")
+    guess = si.sad()
+    with rijk.FockBuilder(0) as fb:
+        fb.set_metric(si.V)
+        fb.set_3c(si.I3, si.n)
+        E64, _, r64 = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess)
+        Et, _, rt = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess, precision=rijk.PREC_MIXED,
+                           converger=rijk.CONV_DIIS_SOSCF, fp64_phase=rijk.PREC_FP64_TC)
+        with pytest.raises(rijk.RijkError) as e:
+            fb.scf(si.H, si.S, si.nocc, si.Enuc, precision=rijk.PREC_MIXED, fp64_phase=rijk.PREC_MIXED)
+        assert e.value.code == rijk.ERR_ARG
+    assert r64["converged"] and rt["converged"] and rt["iterations_mixed"] > 0
+    assert abs(Et - E64) < 1e-9, (Et, E64)
