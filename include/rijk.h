@@ -252,7 +252,8 @@ typedef struct {
  * closing diagonalisation, src/SCF.cpp:178).  H and S are n x n host
  * arrays; n_c occupied orbitals; the core-Hamiltonian guess (or opts' guess) starts it.
  * Diagonalisation, the converger's algebra and the energy are FP64 on the device.  MO (optional, n x n host) receives the orbitals, one per row, as the
- * reference's MO_VEC; E as in src/SCF.cpp:134. */
+ * reference's MO_VEC; E as in src/SCF.cpp:134.  The call's device work buffers, about
+ * (16 + 2 diis_size) n^2 doubles, stay with the context for the next call until rijk_destroy. */
 int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long n_c, double e_nuc, const rijk_scf_opts_t* opts,
              double* MO, rijk_scf_result_t* result);
 

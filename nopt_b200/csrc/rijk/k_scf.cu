@@ -464,13 +464,16 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   const int m_max = o.diis_size;
   constexpr long kMixedRows = 192;  // orbitals one mixed build takes
 
-  DeviceBuf dH, dS, dX, dF, dFex, dD, dDn, dC, dJ, dK, dT1, dT2, dE, dW, dU, work, info, red, out, ring_F, ring_E;
-  DeviceBuf dV, dPur, dInfo2;  // occupied eigenvectors (X basis), purification scalars, Cholesky infos
-  auto cleanup = [&]() {
-    DeviceBuf* all[] = {&dH, &dS, &dX, &dF, &dFex, &dD, &dDn, &dC, &dJ, &dK, &dT1, &dT2, &dE, &dW, &dU,
-                        &work, &info, &red, &out, &ring_F, &ring_E, &dV, &dPur, &dInfo2};
-    for (DeviceBuf* b : all) release(*b);
-  };
+  // Work buffers live in the context between calls (grown as needed, freed by rijk_destroy): an SCF
+  // call then makes no cudaMalloc / cudaFree, whose frees synchronise the device.
+  DeviceBuf* wb = ctx->scf;
+  DeviceBuf &dH = wb[0], &dS = wb[1], &dX = wb[2], &dF = wb[3], &dFex = wb[4], &dD = wb[5], &dDn = wb[6],
+            &dC = wb[7], &dJ = wb[8], &dK = wb[9], &dT1 = wb[10], &dT2 = wb[11], &dE = wb[12], &dW = wb[13],
+            &dU = wb[14], &work = wb[15], &info = wb[16], &red = wb[17], &out = wb[18], &ring_F = wb[19],
+            &ring_E = wb[20];
+  // occupied eigenvectors (X basis), purification scalars, Cholesky infos
+  DeviceBuf &dV = wb[21], &dPur = wb[22], &dInfo2 = wb[23];
+  auto cleanup = [&]() {};  // nothing to free: the buffers stay with the context
   const size_t b_nn = nn * sizeof(double);
   if ((rc = ensure(ctx, dH, b_nn, "scf H")) || (rc = ensure(ctx, dS, b_nn, "scf S")) ||
       (rc = ensure(ctx, dX, b_nn, "scf X")) || (rc = ensure(ctx, dF, b_nn, "scf F")) ||
@@ -675,7 +678,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
 
   if (o.guess_dm && o.guess_rows && o.guess_nrows > 0) {
     // start from the given density: one build with its factor rows, then diagonalise
-    DeviceBuf dR;
+    DeviceBuf& dR = wb[26];
     if ((rc = ensure(ctx, dR, static_cast<size_t>(o.guess_nrows) * n * sizeof(double), "scf guess rows"))) {
       cleanup();
       return rc;
@@ -700,7 +703,6 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
       rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf guess");
     }
-    release(dR);
     if (rc) {
       cleanup();
       return rc;
@@ -871,7 +873,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     const int mvec = o.lbfgs_vectors > 0 ? o.lbfgs_vectors
                                          : static_cast<int>(std::min<long>(nm, std::min(20, o.max_iter)));
     const size_t nmm = static_cast<size_t>(nm) * nm;
-    DeviceBuf lb, qrw;
+    DeviceBuf &lb = wb[24], &qrw = wb[25];
     int lw_chol = 0;
     if ((rc = ensure(ctx, lb, ((2 * static_cast<size_t>(mvec) + 8) * dimc + 2 * nmm) * sizeof(double),
                      "scf L-BFGS"))) {
@@ -891,21 +893,14 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     double* Rq = Fmo + nmm;                   // rotation, then its orthonormal columns
     cudaMemsetAsync(lb.p, 0, lb.bytes, s);
     if (cusolverDnDpotrf_bufferSize(cs, CUBLAS_FILL_MODE_UPPER, nmi, Fmo, nmi, &lw_chol) != CUSOLVER_STATUS_SUCCESS) {
-      release(lb);
       return fail(RIJK_ERR_SOLVER, "Cholesky buffer query failed");
     }
     const int lwq = std::max(lw_chol, 1);
     if ((rc = ensure(ctx, qrw, static_cast<size_t>(lwq) * sizeof(double), "scf QR work"))) {
-      release(lb);
       cleanup();
       return rc;
     }
     double* pQw = static_cast<double*>(qrw.p);
-    auto fail2 = [&](int code, const char* msg) {
-      release(lb);
-      release(qrw);
-      return fail(code, msg);
-    };
     const unsigned gd = grid_of(dim);
     // no first-iteration diagonalisation after a start from a Fock matrix's own orbitals
     const bool guess_diag = soscf_from_diis || (o.guess_dm && o.guess_rows && o.guess_nrows > 0);
@@ -917,8 +912,6 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     for (int it = 0; it < o.max_iter - it_used; ++it) {
       auto ta = now();
       if ((rc = build(prec))) {
-        release(lb);
-        release(qrw);
         cleanup();
         return rc;
       }
@@ -934,8 +927,6 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       }
       cudaMemcpyAsync(hout.data(), pOut, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
       if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf iteration")) || (rc = check_device_error(ctx))) {
-        release(lb);
-        release(qrw);
         cleanup();
         return rc;
       }
@@ -972,7 +963,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       }
       auto tc = now();
       if (it == 0 && !guess_diag) {  // first iteration: plain diagonalisation (src/SCF.cpp:160-166)
-        if (diag(pF, true) != RIJK_OK) return fail2(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
+        if (diag(pF, true) != RIJK_OK) return fail(RIJK_ERR_SOLVER, "syevd of the Fock matrix failed");
         density(pDn);
         reduce(DiffSqF{pDn, pD}, nn, 0, 5);
         std::swap(pD, pDn);
@@ -1021,7 +1012,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       for (int pass = 0; pass < 2; ++pass) {
         cublasDsyrk(cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nmi, nmi, &one, Rq, nmi, &zero, Fmo, nmi);  // A^T A
         if (cusolverDnDpotrf(cs, CUBLAS_FILL_MODE_UPPER, nmi, Fmo, nmi, pQw, lwq, pInfo) != CUSOLVER_STATUS_SUCCESS)
-          return fail2(RIJK_ERR_SOLVER, "Cholesky factorisation of the rotation's Gram matrix failed");
+          return fail(RIJK_ERR_SOLVER, "Cholesky factorisation of the rotation's Gram matrix failed");
         cublasDtrsm(cb, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nmi, nmi, &one,
                     Fmo, nmi, Rq, nmi);  // A U^-1
       }
@@ -1034,8 +1025,6 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       E_old = E;
       t_diag += msec(td, now());
     }
-    release(lb);
-    release(qrw);
   }
   const auto t_loop1 = std::chrono::steady_clock::now();
   // The energy is the last FP64 build's, as the reference reports it (src/SCF.cpp:134-156): a run

@@ -298,6 +298,7 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
                        &ctx->stageK, &ctx->Dt, &ctx->w,     &ctx->Jpart, &ctx->MOp,    &ctx->XT,
                        &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab, &ctx->Xs, &ctx->Xe};
   for (DeviceBuf* b : bufs) release(*b);
+  for (DeviceBuf& b : ctx->scf) release(b);
   if (ctx->cublas) cublasDestroy(ctx->cublas);
   if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
   if (ctx->copy_stream) {

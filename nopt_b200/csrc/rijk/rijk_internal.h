@@ -78,6 +78,7 @@ struct rijk_ctx {
   rijk::DeviceBuf Xs;       // int8 digits of X^T for the tensor-core FP64 exchange: npad2 rows of kdim/32
                             // blocks of 8 digits x 32 bytes
   rijk::DeviceBuf Xe;       // their row exponents, parts x npad2
+  rijk::DeviceBuf scf[32];  // rijk_scf's work buffers, kept between calls
 
   rijk_stats_t stats{};
   std::string last_error;
