@@ -6,7 +6,7 @@
 //     X[nu][k] = 2^e(r,nu) * sum_{s=0}^{7} d_s[nu][k] 2^{-7(s+1)},   d_s integer in [-64, 64],
 // with e chosen so that max_k |X[nu][k]| / 2^e < 1/2 (k_slice_x).  The digits are exact: each
 // step scales by 2^7, rounds to the nearest integer and keeps the exact remainder, so the value
-// left after 8 digits is below 2^-57 of the row maximum.  Then
+// left after 8 digits is at most 2^-57 of 2^e, which is below 2^-55 of the row maximum.  Then
 //     K_mu,nu = 2^(e_mu + e_nu) sum_g 2^{-7(g+2)} sum_{s+t=g} (d_s[mu] . d_t[nu]),
 // where every (d_s . d_t) is an exact s32 tensor-core sum (|d_s d_t| <= 4096; a part spans at
 // most 65504 k, and a group sums at most 8 pairs: 8 * 4096 * 65504 < 2^31 - 1).  The groups g < 8
