@@ -30,15 +30,13 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernels,
-# from one ncu capture each (profiles/k_xform_f64_h2o16_dz.md, profiles/k_xform_tc_syrk_tc_h2o16_dz.md).
-# dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/fp64_exchange_h2o16_dz.md,
-# profiles/mixed_kernels_h2o16_dz.md)
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernels at
+# (H2O)16 cc-pVDZ, from one ncu capture of each (summaries under profiles/)
 NCU_TRAFFIC = {("h2o16_dz", "xform_f64"): 1.277529e9 + 0.437618e9,
                ("h2o16_dz", "syrk_f64"): 0.457111e9 + 0.092111e9,
                ("h2o16_dz", "xform_tc"): 0.639337e9 + 0.202236e9,
                ("h2o16_dz", "syrk_tc"): 0.228261e9 + 0.030061e9,
-               ("h2o16_dz", "syrk_i8"): 0.968671e9 + 0.089102e9,
+               ("h2o16_dz", "syrk_i8"): 0.970246e9 + 0.088795e9,
                ("h2o16_dz", "coulomb_w_mixed"): 0.639341e9 + 0.004234e9,
                ("h2o16_dz", "coulomb_j_mixed"): 0.638610e9 + 0.010762e9}
 WORKLOAD_NAMES = {"h2o6_dz": "(H2O)6 cc-pVDZ/cc-pVDZ-JKFIT", "h2o16_dz": "(H2O)16 cc-pVDZ/cc-pVDZ-JKFIT",
