@@ -398,7 +398,7 @@ def main():
 
     peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
-    # FP64 peak: the box's own cuBLAS DGEMM (the driver's peak file has no FP64 figure)
+    # FP64 peak: cuBLAS DGEMM measured on this GPU (the measured-peaks file has no FP64 figure)
     a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
     b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
     torch.matmul(a, b)

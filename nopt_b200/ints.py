@@ -28,7 +28,7 @@ def lib():
     if _LIB is None:
         path = os.path.join(_HERE, "libgto_ints.so")
         if not os.path.exists(path):
-            raise RuntimeError("libgto_ints.so is not built; run __graft_entry__.build()")
+            raise RuntimeError("libgto_ints.so is not built; run python nopt_b200/build.py")
         L = ctypes.CDLL(path)
         L.gto_basis_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _dp]
         L.gto_basis_destroy.argtypes = [ctypes.c_void_p]

@@ -94,7 +94,7 @@ def lib():
     if _LIB is None:
         path = lib_path()
         if not os.path.exists(path):
-            raise RuntimeError("librijk.so is not built (run __graft_entry__.build()); there is no CPU fallback")
+            raise RuntimeError("librijk.so is not built (run python nopt_b200/build.py); there is no CPU fallback")
         L = ctypes.CDLL(path)
         P = ctypes.POINTER
         L.rijk_create.argtypes = [P(_vp), ctypes.c_int]

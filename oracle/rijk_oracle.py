@@ -1,7 +1,7 @@
 """CPU oracle for the RI-JK Fock build — TEST INFRASTRUCTURE ONLY.
 
-This module is the checker.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
-baseline leg may import it; the product path (nopt_b200/, librijk.so) never does.
+It is the oracle the tests compare against.  Only tests/, __graft_entry__.smoke() and bench.py's
+CPU baseline leg may import it; the product path (nopt_b200/, librijk.so) never does.
 
 It restates, in numpy (float64 throughout, OpenBLAS dgemm underneath), the reference's
 algorithm for the hot path in the reference's own operation order:
