@@ -1,19 +1,22 @@
-"""Benchmark of the RI-JK Fock build on B200: Fock builds per second.
+"""Benchmark of the RI-JK Fock build on B200: Fock builds per second and SCF time.
 
-Workload (default): water 16-mer (H2O)16, cc-pVDZ / cc-pVDZ-JKFIT (n = 384, naux = 1856,
-nocc = 80), seeded jittered 4x2x2 lattice.  A step is one Fock build (J and K) over the
-resident fitted tensor B (1.3 GB, larger than the 126 MB L2, so no flush is needed between
+Workload (default): water 32-mer (H2O)32, cc-pVTZ / cc-pVTZ-JKFIT (n = 1856, naux = 4448,
+nocc = 160), seeded jittered 4x4x2 lattice.  A step is one Fock build (J and K) over the
+resident fitted tensor B (63 GB, far larger than the 126 MB L2, so no flush is needed between
 steps).  `value` is device-timed FP64 builds/s with the inputs in HBM; `e2e` is the same
-metric through the drop-in C ABI call (host D and C in, host J and K out); the mixed
-precision form and the SCF time to convergence are reported beside it.
+metric through the drop-in C ABI call (pinned host D and C in, host J and K out; `e2e_pageable`
+with plain pageable arrays, as the reference passes them); the mixed-precision form
+(`mixed.value`, `mixed.speedup_vs_fp64`) and the SCF time to convergence are reported beside it.
+The (H2O)16 cc-pVDZ workload and a CPU SCF time at (H2O)6 come as extra keys.
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload NAME]
 
 With N > 1 (torchrun) every rank runs an independent replica of the workload (the Fock
 build of one molecule is a one-GPU problem): weak scaling, value = total builds/s.
-`--impl reference` times the reference's CPU algorithm (the oracle's restatement of
-DM_to_F_transform_RI in the reference's dgemm order; the reference itself does not build
-here) on all host threads.
+`--impl reference` times the reference's CPU algorithm on all host threads: the oracle's
+restatement of DM_to_F_transform_RI in the reference's dgemm order (the reference itself does not
+build here), as whole builds where its full-square RI_AA fits in host memory, else one aux slice
+of the build per step (every stage's share of that slice; see oracle sliced_step).
 """
 import argparse
 import json
@@ -50,11 +53,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="h2o16_dz")
+    ap.add_argument("--workload", default="h2o32_tz")
+    ap.add_argument("--extra", default="h2o16_dz", help="second workload reported under its own key ('none': skip)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-scf", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-slices", type=int, default=12,
+                    help="aux slices of the CPU arm when the full-square RI_AA does not fit host memory")
     ap.add_argument("--setup", default="gpu", choices=["gpu", "host"],
                     help="gpu: integrals on the device (rijk_set_basis); host: host integrals + rijk_set_3c")
     ap.add_argument("--shard", default="replicas", choices=["replicas", "q"],
@@ -162,24 +168,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_builds_per_s(si, DM, MO, budget_s):
-    """The oracle's restatement of DM_to_F_transform_RI on the host (all threads)."""
+# ------------------------------------------------------------------ CPU arm ------
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import rijk_oracle as O
+    return O
+
+
+def _blas_threads():
     from threadpoolctl import threadpool_info
-    RI = O.unpack_3c(si.I3, si.n)
-    Vm05, _ = O.s05_calc(si.V)
-    O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)  # warm
-    t0 = time.perf_counter()
-    k = 0
-    while True:
-        O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)
-        k += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or k >= 50:
-            break
-    threads = max([p.get("num_threads", 1) for p in threadpool_info()] or [1])
-    return k / el, threads, "%d full builds in NOPT layout (RI_AA %.2f GB), %.1f s" % (k, RI.nbytes / 1e9, el)
+    return max([p.get("num_threads", 1) for p in threadpool_info()] or [1])
 
 
 def workload_shape(workload, seed):
@@ -194,14 +192,6 @@ def workload_shape(workload, seed):
     return ints.Basis.for_molecule(ob, mol).nbf, ints.Basis.for_molecule(ab, mol).nbf, mol.nelec // 2
 
 
-def host_bytes(workload, seed):
-    """Host bytes of (packed (mu nu|P), and that plus the CPU arm's arrays: the oracle's full-square
-    RI_AA in NOPT's layout and its two half-transformed copies)."""
-    n, naux, nocc = workload_shape(workload, seed)
-    packed = n * (n + 1) // 2 * naux * 8
-    return packed, packed + n * n * naux * 8 + 2 * nocc * n * naux * 8
-
-
 def host_available():
     with open("/proc/meminfo") as f:
         for line in f:
@@ -210,48 +200,246 @@ def host_available():
     return 0
 
 
-def cpu_arm_fits(workload, seed):
-    """None when the CPU arm fits in 70% of the host's available memory, else the reason it does not."""
-    _, need = host_bytes(workload, seed)
+def cpu_arm_plan(workload, seed, nslices):
+    """("full", bytes) when the reference's full-square RI_AA and its half-transformed copies fit in
+    70% of the host's available memory; ("sliced", bytes) when one aux slice and RI_CA do;
+    ("unavailable", reason) otherwise."""
+    n, naux, nocc = workload_shape(workload, seed)
+    full = n * (n + 1) // 2 * naux * 8 + n * n * naux * 8 + 2 * nocc * n * naux * 8
     avail = host_available()
-    if need <= 0.7 * avail:
-        return None
-    return ("the CPU arm needs %.0f GB of host memory (RI_AA in NOPT's layout and its copies), %.0f GB are available"
-            % (need / 1e9, avail / 1e9))
+    if full <= 0.7 * avail:
+        return "full", full
+    sliced = nocc * n * naux * 8 + 2.2 * n * n * (naux / max(nslices, 1)) * 8 + n * n * 8 * 4
+    if sliced <= 0.7 * avail:
+        return "sliced", sliced
+    return "unavailable", ("the CPU arm needs %.0f GB of host memory even with %d aux slices; %.0f GB are available"
+                           % (sliced / 1e9, nslices, avail / 1e9))
 
 
-def run_reference(args, rank):
-    if rank != 0:
-        return
-    why = cpu_arm_fits(args.workload, args.seed)
-    if why:
-        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
-        return
-    si, tint, (ob, ab) = build_system(args.workload, args.seed)
-    DM, MO = core_guess(si)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import rijk_oracle as O
-    from threadpoolctl import threadpool_info
+def cpu_full(si, DM, MO, steps=None, warmup=1, budget_s=None):
+    """Whole builds of the oracle's DM_to_F_transform_RI (NOPT layout) on all host threads: either
+    `steps` builds after `warmup`, or as many as fit in budget_s.  Returns (builds/s, builds, seconds, note)."""
+    O = _oracle()
     RI = O.unpack_3c(si.I3, si.n)
     Vm05, _ = O.s05_calc(si.V)
-    for _ in range(max(args.warmup, 0)):
+    for _ in range(max(warmup, 1)):
         O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    k = 0
+    while True:
         O.dm_to_f_transform_ri(RI, Vm05, DM, MO, si.nocc, si.n)
+        k += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and k >= steps) or (steps is None and (el > budget_s or k >= 50)):
+            break
+    return k / el, k, el, "%d whole builds in NOPT layout (RI_AA %.2f GB) after %d untimed" % (
+        k, RI.nbytes / 1e9, max(warmup, 1))
+
+
+def cpu_sliced(si, DM, MO, nslices, steps, warmup):
+    """The oracle's aux-sliced restatement of DM_to_F_transform_RI: untimed set-up (V^-1/2, and
+    RI_CA and the Coulomb coefficients from every raw slice of (mu nu|P) computed by the host
+    integral engine), then `steps` timed repetitions of one slice's share of the build.  A slice
+    of s of the naux aux functions carries s / naux of every stage's products, so builds/s =
+    (s / naux) / (seconds per slice step).  Returns (builds/s, steps, seconds, note, set-up s)."""
+    from nopt_b200 import ints
+    O = _oracle()
+    n, naux, nocc = si.n, si.naux, si.nocc
+    t0 = time.perf_counter()
+    V = si.V if si.V is not None else ints.coulomb_2c(si.aux)
+    Vm05, _ = O.s05_calc(V)
+    bounds = ints.aux_slice_bounds(si.aux, nslices)
+    mid = len(bounds) // 2
+    keep = {}
+
+    def raw(p0, p1):
+        A = ints.coulomb_3c_aux_range(si.orb, si.aux, p0, p1)
+        if (p0, p1) == bounds[mid]:
+            keep["A"] = A
+        return A
+
+    RI_CA, RI_Jv = O.sliced_setup(raw, bounds, Vm05, DM, MO, nocc, n)
+    p0, p1 = bounds[mid]
+    A = keep.pop("A")
+    t_setup = time.perf_counter() - t0
+    for _ in range(max(warmup, 1)):
+        O.sliced_step(A, p0, p1, RI_CA, RI_Jv, Vm05, DM, MO, nocc, n)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.sliced_step(A, p0, p1, RI_CA, RI_Jv, Vm05, DM, MO, nocc, n)
     el = time.perf_counter() - t0
-    v = args.steps / el
-    threads = max([p.get("num_threads", 1) for p in threadpool_info()] or [1])
+    frac = (p1 - p0) / naux
+    note = ("%d steps, each the share of aux slice [%d, %d) (%d of %d aux functions, %.4f of a build) of every stage "
+            "of the reference's build, in its dgemm order; the full-square RI_AA (%.0f GB) does not fit in host "
+            "memory, so it is held one slice (%.1f GB) at a time and RI_CA (%.1f GB) whole" %
+            (steps, p0, p1, p1 - p0, naux, frac, n * n * naux * 8 / 1e9, A.nbytes / 1e9, RI_CA.nbytes / 1e9))
+    return frac * steps / el, steps, el, note, t_setup
+
+
+def config_of(workload, n, naux, nocc, world, sharded, seed):
+    """The `config` object of both arms' JSON lines."""
+    nt = (n + 63) // 64
+    bytes_b = naux * (nt * (nt + 1) // 2) * 4096 * 8
+    name = WORKLOAD_NAMES.get(workload)
+    if name is None:
+        name = ("synthetic " + workload[5:].replace(",", " ") + " (random packed B ~ N(0,1) e^-|mu-nu|/n)"
+                if workload.startswith("rand:") else workload)
+    return {"workload": name, "n": n, "naux": naux, "nocc": nocc,
+            "parallelism": ("aux-sharded x%d" % world) if sharded else ("replicas x%d" % world if world > 1 else "single"),
+            "l2": "inputs larger than L2 (B = %.2f GB)" % (bytes_b / 1e9), "seed": seed}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    n, naux, nocc = workload_shape(args.workload, args.seed)
+    cfg = config_of(args.workload, n, naux, nocc, world, args.shard == "q" and world > 1, args.seed)
+    mode, need = cpu_arm_plan(args.workload, args.seed, args.cpu_slices)
+    if mode == "unavailable":
+        print(json.dumps({"impl": "reference", "unavailable": need}), flush=True)
+        return
+    si, tint, (ob, ab) = build_system(args.workload, args.seed, ri_integrals=(mode == "full"))
+    DM, MO = core_guess(si)
+    setup = None
+    if mode == "full":
+        v, k, el, note = cpu_full(si, DM, MO, steps=args.steps, warmup=args.warmup)
+    else:
+        v, k, el, note, setup = cpu_sliced(si, DM, MO, args.cpu_slices, args.steps, args.warmup)
+    threads = _blas_threads()
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "builds/s", "n_gpus": 0, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD_NAMES.get(args.workload, args.workload), "n": si.n, "naux": si.naux,
-                      "nocc": si.nocc},
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
            "cpu_baseline": {"value": v, "unit": "builds/s", "cores": threads, "kind": "port",
-                            "sample": "%d builds of the reference's dgemm sequence (oracle restatement; the reference "
-                                      "needs libint2/Eigen/Boost/LAPACKE, absent here)" % args.steps},
-           "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                            "sample": note + " (oracle restatement; the reference needs libint2/Eigen/Boost/LAPACKE, "
+                                             "absent here)"},
+           "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "setup_s": {"host_integrals": tint, "sliced_setup": setup}}
     print(json.dumps(out), flush=True)
+
+
+def cpu_baseline_for(si, DM, MO, workload, seed, nslices, budget_s):
+    """cpu_baseline object of our arm: whole builds within budget_s where they fit, else two slice steps."""
+    mode, need = cpu_arm_plan(workload, seed, nslices)
+    if mode == "unavailable":
+        return {"skipped": need}
+    if mode == "full":
+        v, k, el, note = cpu_full(si, DM, MO, budget_s=budget_s)
+    else:
+        v, k, el, note, _ = cpu_sliced(si, DM, MO, nslices, 2, 1)
+    return {"value": v, "unit": "builds/s", "cores": _blas_threads(), "kind": "port", "sample": note}
+
+
+# ------------------------------------------------------------------ GPU arm ------
+def extra_workload(name, seed, dev, steps, want_cpu, budget_s):
+    """A second workload on a fresh context: FP64 and mixed builds/s (device-timed), e2e through
+    rijk_fock, SCF times, the adjoint's time, and the CPU arm's builds/s."""
+    import ctypes
+    import torch
+    from nopt_b200 import rijk
+    si, _, _ = build_system(name, seed, ri_integrals=True)
+    DM, MO = core_guess(si)
+    n, nocc = si.n, si.nocc
+    stream = torch.cuda.current_stream(dev)
+    out = {"workload": WORKLOAD_NAMES.get(name, name), "n": n, "naux": si.naux, "nocc": nocc}
+    with rijk.FockBuilder(dev.index) as fb:
+        fb.set_stream(stream.cuda_stream)
+        fb.set_basis(si.orb, si.aux, rijk.METRIC_INVSQRT)
+        dD = torch.from_numpy(DM).to(dev)
+        dMO = torch.from_numpy(MO[:nocc].copy()).to(dev)
+        dJ = torch.empty((n, n), dtype=torch.float64, device=dev)
+        dK = torch.empty((n, n), dtype=torch.float64, device=dev)
+
+        def timed(prec):
+            for _ in range(3):
+                fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            return e0.elapsed_time(e1) / steps
+
+        ms64 = timed(rijk.PREC_FP64)
+        msmx = timed(rijk.PREC_MIXED)
+        out["fp64"] = {"value": 1e3 / ms64, "unit": "builds/s", "ms_per_step": ms64}
+        out["mixed"] = {"value": 1e3 / msmx, "unit": "builds/s", "ms_per_step": msmx, "speedup_vs_fp64": ms64 / msmx}
+        hD = torch.from_numpy(DM).pin_memory()
+        hMO = torch.from_numpy(MO[:nocc].copy()).pin_memory()
+        hJ = torch.empty((n, n), dtype=torch.float64).pin_memory()
+        hK = torch.empty((n, n), dtype=torch.float64).pin_memory()
+        P = ctypes.POINTER(ctypes.c_double)
+        pD, pMO, pJ, pK = [ctypes.cast(t.data_ptr(), P) for t in (hD, hMO, hJ, hK)]
+        L = rijk.lib()
+        fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
+        out["e2e"] = {"value": steps / (time.perf_counter() - t0), "unit": "builds/s",
+                      "h2d_bytes_per_step": int((n * n + nocc * n) * 8), "d2h_bytes_per_step": int(2 * n * n * 8)}
+        guess = si.sad()
+        scf = {}
+        fb.scf(si.H, si.S, nocc, si.Enuc, guess=guess)  # untimed first call
+        for key, prec, conv in (("fp64", rijk.PREC_FP64, rijk.CONV_DIIS),
+                                ("diis_mixed_then_soscf_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF)):
+            best = None
+            for _ in range(3):
+                t0 = time.perf_counter()
+                E, _, r = fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, guess=guess, converger=conv)
+                t = time.perf_counter() - t0
+                if best is None or t < best[0]:
+                    best = (t, E, r)
+            scf[key] = {"seconds": best[0], "energy": best[1], "iterations": best[2]["iterations"],
+                        "iterations_mixed": best[2]["iterations_mixed"]}
+        scf["diis_mixed_then_soscf_fp64"]["abs_dE_vs_fp64"] = abs(scf["diis_mixed_then_soscf_fp64"]["energy"] -
+                                                                  scf["fp64"]["energy"])
+        out["scf"] = scf
+        # the adjoint (rijk_grad) at the converged FP64 orbitals: E, dE/dC, dE/d(P|mu nu), dE/d(P|Q)
+        E, MOc, _ = fb.scf(si.H, si.S, nocc, si.Enuc, guess=guess)
+        fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
+        out["grad"] = {"ms": 1e3 * (time.perf_counter() - t0) / 3,
+                       "what": "rijk_grad wall time through the C ABI: E, dE/dC, dE/d(P|mu nu) (packed) and dE/d(P|Q), "
+                               "host outputs"}
+    if want_cpu:
+        out["cpu_baseline"] = cpu_baseline_for(si, DM, MO, name, seed, 12, budget_s)
+        if "value" in out["cpu_baseline"]:
+            out["ratio_e2e_vs_cpu"] = out["e2e"]["value"] / out["cpu_baseline"]["value"]
+    return out
+
+
+def scf_cpu_small(seed, dev):
+    """SCF time to convergence of the reference's algorithm on the host (the oracle's RHF with its
+    restated Fock build, whole builds in NOPT layout, all threads) beside rijk_scf on the GPU, for the
+    (H2O)6 cc-pVDZ/cc-pVDZ-JKFIT workload the reference runs as-is; the same SAD start and the same
+    criterion (density RMS change < 1e-10)."""
+    from nopt_b200 import ints, rijk
+    O = _oracle()
+    si, _, _ = build_system("h2o6_dz", seed, ri_integrals=True)
+    RI = O.unpack_3c(si.I3, si.n)
+    guess = si.sad()
+    t0 = time.perf_counter()
+    Vm05, _ = O.s05_calc(si.V)
+    Ec, _, _, _, itc = O.scf_rhf(si.S, si.H, RI, Vm05, si.nocc, si.Enuc, conv_dm=1e-10, guess=guess)
+    tc = time.perf_counter() - t0
+    with rijk.FockBuilder(dev.index) as fb:
+        fb.set_basis(si.orb, si.aux, rijk.METRIC_INVSQRT)
+        fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess)
+        best = None
+        for _ in range(3):
+            t0 = time.perf_counter()
+            Eg, _, r = fb.scf(si.H, si.S, si.nocc, si.Enuc, guess=guess)
+            t = time.perf_counter() - t0
+            best = (t, Eg, r["iterations"]) if best is None or t < best[0] else best
+    return {"workload": WORKLOAD_NAMES["h2o6_dz"], "cpu_seconds": tc, "cpu_builds": itc + 2, "cpu_energy": Ec,
+            "cpu_cores": _blas_threads(), "gpu_seconds": best[0], "gpu_builds": best[2], "gpu_energy": best[1],
+            "abs_dE": abs(Ec - best[1]), "speedup": tc / best[0],
+            "note": "CPU: oracle RHF/DIIS with the restated DM_to_F_transform_RI (V^-1/2 set-up included, integrals "
+                    "not); GPU: rijk_scf FP64 DIIS after rijk_set_basis, fastest of three"}
 
 
 def main():
@@ -267,7 +455,7 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
-        run_reference(args, rank)
+        run_reference(args, rank, world)
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -278,17 +466,15 @@ def main():
     synthetic = args.workload.startswith("rand:")
     if synthetic:  # no basis: integrals come from the seeded generator, set up through rijk_set_3c
         args.setup, args.no_scf = "host", True
-    # host RI integrals only where something needs them: the host set-up path or the CPU baseline,
-    # and the CPU baseline only where its arrays fit in host memory
     want_cpu = not args.no_cpu and rank == 0 and world == 1
-    cpu_skip = cpu_arm_fits(args.workload, args.seed) if want_cpu else None
-    if cpu_skip:
-        want_cpu = False
+    mode, _ = cpu_arm_plan(args.workload, args.seed, args.cpu_slices) if want_cpu else ("none", None)
     if args.setup == "host":
-        packed, _ = host_bytes(args.workload, args.seed)
+        n_, naux_, _ = workload_shape(args.workload, args.seed)
+        packed = n_ * (n_ + 1) // 2 * naux_ * 8
         if packed > 0.7 * host_available():
             raise SystemExit("--setup host needs %.0f GB of host memory for (mu nu|P); use --setup gpu" % (packed / 1e9))
-    need_host_ri = args.setup == "host" or want_cpu
+    # host RI integrals only where something needs them: the host set-up path or a whole-build CPU arm
+    need_host_ri = args.setup == "host" or mode == "full"
     si, tint, (ob, ab) = build_system(args.workload, args.seed, ri_integrals=need_host_ri)
     DM, MO = core_guess(si)
     n, naux, nocc = si.n, si.naux, si.nocc
@@ -351,35 +537,50 @@ def main():
     launches = st["kernels_last_fock"] * args.steps
     value = (1 if sharded else world) * 1e3 / ms
 
-    # end to end through the drop-in call: pinned host D, C in; host J, K out
+    # end to end through the drop-in call: host D, C in; host J, K out.  Pinned buffers, and
+    # plain pageable arrays as the reference passes them (J and K are new[]'d per call there,
+    # src/molecule.cpp:4409-4415).
+    import ctypes
+    P = ctypes.POINTER(ctypes.c_double)
+    L = rijk.lib()
+
+    def e2e(hD, hMO, hJ, hK, steps):
+        pD, pMO, pJ, pK = [ctypes.cast(p, P) for p in (hD, hMO, hJ, hK)]
+        for _ in range(2):
+            fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
+            if sharded:  # the host matrices of all ranks summed through the GPU
+                Jt = torch.from_numpy(np.ctypeslib.as_array(ctypes.cast(hJ, P), (n, n)))
+                Kt = torch.from_numpy(np.ctypeslib.as_array(ctypes.cast(hK, P), (n, n)))
+                tj, tk = Jt.to(dev), Kt.to(dev)
+                dist.all_reduce(tj)
+                dist.all_reduce(tk)
+                Jt.copy_(tj.cpu())
+                Kt.copy_(tk.cpu())
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        t = e0.elapsed_time(e1) / steps
+        if dist is not None:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
     hD = torch.from_numpy(DM).pin_memory()
     hMO = torch.from_numpy(MO[:nocc].copy()).pin_memory()
     hJ = torch.empty((n, n), dtype=torch.float64).pin_memory()
     hK = torch.empty((n, n), dtype=torch.float64).pin_memory()
-    import ctypes
-    P = ctypes.POINTER(ctypes.c_double)
-    pD, pMO, pJ, pK = [ctypes.cast(t.data_ptr(), P) for t in (hD, hMO, hJ, hK)]
-    L = rijk.lib()
-    for _ in range(2):
-        fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        fb._check(L.rijk_fock(fb._h, pD, pMO, nocc, pJ, pK, rijk.PREC_FP64))
-        if sharded:  # the host matrices of all ranks summed through the GPU
-            tj, tk = hJ.to(dev, non_blocking=True), hK.to(dev, non_blocking=True)
-            dist.all_reduce(tj)
-            dist.all_reduce(tk)
-            hJ.copy_(tj, non_blocking=True)
-            hK.copy_(tk, non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ms_e2e = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = e2e(hD.data_ptr(), hMO.data_ptr(), hJ.data_ptr(), hK.data_ptr(), args.steps)
+    pgD, pgMO = np.ascontiguousarray(DM), np.ascontiguousarray(MO[:nocc])
+    pgJ, pgK = np.empty((n, n)), np.empty((n, n))
+    psteps = max(3, args.steps // 4)
+    ms_e2e_pg = e2e(pgD.ctypes.data, pgMO.ctypes.data, pgJ.ctypes.data, pgK.ctypes.data, psteps)
 
     # per-kernel device times (events around each launch on the launching stream)
     def stage_times(prec, reps=5):
@@ -402,6 +603,7 @@ def main():
     a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
     b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
     torch.matmul(a, b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     best = 1e9
     for _ in range(3):
         e0.record(stream)
@@ -449,13 +651,12 @@ def main():
         K64 = dK.cpu().numpy()
         mstages = stage_times(rijk.PREC_MIXED)
         mtop = max(mstages, key=mstages.get)
-        mixed = {"value": (1 if sharded else world) * 1e3 / msm, "unit": "builds/s", "ms_per_step": msm, "speedup_vs_fp64": ms / msm,
+        mixed = {"value": (1 if sharded else world) * 1e3 / msm, "unit": "builds/s", "ms_per_step": msm,
+                 "speedup_vs_fp64": ms / msm,
                  "max_abs_dK_vs_fp64": float(np.max(np.abs(Km - K64))),
                  "exchange_energy_err": float(abs(np.sum(DM * (Km - K64)))),
                  "stage_ms": mstages, "top_kernel": mtop, "clocks": mclk.summary(),
                  "gpu_launches": fb.stats()["kernels_last_fock"] * args.steps}
-        if mtop in ("xform_tc", "syrk_tc"):
-            mixed["traffic"] = NCU_TRAFFIC.get((args.workload, mtop))
         # every mixed kernel against its roofline; the tensor peak is the sustained (power-capped)
         # figure when the clocks sampled during the mixed timing show the power cap, else the burst one
         capped = "sw_power_cap" in (mclk.summary().get("reasons") or [])
@@ -464,12 +665,14 @@ def main():
         npad2 = ((npad + 127) // 128) * 128
         nb = npad2 // 128
         flops = {"xform_tc": 3 * 2.0 * noccp * npad2 * npad2 * naux,
-                 "syrk_tc": 3 * 2.0 * naux * noccp * 128 * 128 * nb * (nb + 1) / 2}
+                 "syrk_tc": 3 * 2.0 * naux * noccp * 128 * 128 * nb * (nb + 1) / 2,
+                 "syrk_tc2": 3 * 2.0 * naux * noccp * 128 * 128 * nb * (nb + 1) / 2}
         mbytes = tile_elems * naux * 4.0  # hi + lo bf16 planes of the stored tiles
         xt_bytes = npad2 * naux * noccp * 4.0  # the split X^T, hi + lo
         ntile2 = nb * 2 * (nb * 2 + 1) // 2
         tbytes = {"xform_tc": mbytes + xt_bytes,  # read the split B once, write X^T once
-                  "syrk_tc": xt_bytes + ntile2 * 4096 * 8.0}  # read X^T once, write K once
+                  "syrk_tc": xt_bytes + ntile2 * 4096 * 8.0,  # read X^T once, write K once
+                  "syrk_tc2": xt_bytes + ntile2 * 4096 * 8.0}
         roofs = {}
         for k, v in mstages.items():
             if k in flops and v > 0:
@@ -529,10 +732,10 @@ def main():
             Dm = Cm.T @ Cm
             J64, K64 = fb.dm_to_f_transform_ri(Dm, Cm, nocc, rijk.PREC_FP64)
             Jmx, Kmx = fb.dm_to_f_transform_ri(Dm, Cm, nocc, rijk.PREC_MIXED)
-            dJ, dK = Jmx - J64, Kmx - K64
+            dJm, dKm = Jmx - J64, Kmx - K64
             E64 = float(np.sum(Dm * (2 * si.H + 2 * J64 - K64))) + si.Enuc
-            rows.append({"iteration": it, "energy_fp64": E64, "max_abs_dJ": float(np.max(np.abs(dJ))),
-                         "max_abs_dK": float(np.max(np.abs(dK))), "dE": float(np.sum(Dm * (2 * dJ - dK)))})
+            rows.append({"iteration": it, "energy_fp64": E64, "max_abs_dJ": float(np.max(np.abs(dJm))),
+                         "max_abs_dK": float(np.max(np.abs(dKm))), "dE": float(np.sum(Dm * (2 * dJm - dKm)))})
             F = si.H + 2 * J64 - K64
         mixed["per_iteration"] = rows
         mixed["per_iteration_note"] = ("FP64 SCF path from the SAD start (plain diagonalisation); at each density the "
@@ -548,19 +751,21 @@ def main():
         t0 = time.perf_counter()
         guess = si.sad()  # superposition of atomic densities (host, once per geometry)
         t_guess = time.perf_counter() - t0
-        for prec in (rijk.PREC_FP64, rijk.PREC_MIXED):  # untimed: first-call set-up of both forms
-            fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, guess=guess)
-        fb.scf(si.H, si.S, nocc, si.Enuc, guess=guess, converger=rijk.CONV_SOSCF)  # untimed first call
-        runs = (("fp64", rijk.PREC_FP64, rijk.CONV_DIIS), ("mixed_then_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS),
+        big = n > 1024
+        fb.scf(si.H, si.S, nocc, si.Enuc, guess=guess)  # untimed first calls (work buffers, solver set-up)
+        fb.scf(si.H, si.S, nocc, si.Enuc, guess=guess, converger=rijk.CONV_SOSCF)
+        runs = [("fp64", rijk.PREC_FP64, rijk.CONV_DIIS), ("mixed_then_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS),
                 ("soscf_fp64", rijk.PREC_FP64, rijk.CONV_SOSCF),
-                ("soscf_mixed_then_fp64", rijk.PREC_MIXED, rijk.CONV_SOSCF),
                 ("diis_mixed_then_soscf_fp64", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF),
-                ("diis_mixed_then_soscf_fp64tc", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF))
+                ("diis_mixed_then_soscf_fp64tc", rijk.PREC_MIXED, rijk.CONV_DIIS_SOSCF)]
+        if not big:
+            runs.insert(3, ("soscf_mixed_then_fp64", rijk.PREC_MIXED, rijk.CONV_SOSCF))
+        reps = 2 if big else 3
         for name, prec, conv in runs:
             # the last variant's FP64-accurate phase uses FP64_TC builds (K on the int8 tensor cores)
             fp64_phase = rijk.PREC_FP64_TC if name.endswith("fp64tc") else rijk.PREC_FP64
             el = None
-            for _ in range(3):  # the fastest of three runs: host-side latencies make single SCF timings noisy
+            for _ in range(reps):  # the fastest of the runs: host-side latencies make single SCF timings noisy
                 torch.cuda.synchronize(dev)
                 t0 = time.perf_counter()
                 E, _, r = fb.scf(si.H, si.S, nocc, si.Enuc, precision=prec, conv_dm_rms=1e-10, guess=guess,
@@ -578,37 +783,43 @@ def main():
                 E64 = E
             else:
                 out[name]["abs_dE_vs_fp64"] = abs(E - E64)
+        out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / min(
+            out[k]["seconds"] for k in out if k.startswith(("mixed", "diis_mixed", "soscf_mixed")))
         out["criterion"] = ("DIIS: density RMS change < 1e-10; SOSCF (the reference's converger): max|4 F_ai| < 1e-7 "
                             "or |dE| < 1e-10; mixed runs switch to FP64 when the DIIS error / max|4 F_ai| < 1e-5; "
                             "diis_mixed_then_soscf_fp64: DIIS over the mixed builds, the SOSCF step and test after "
                             "the switch")
         out["start"] = "superposition of atomic densities (%.2f s on the host, not in the SCF time)" % t_guess
-        out["timing"] = ("wall time of rijk_scf, the fastest of three runs (ms_inside: the library's own clock of "
+        out["timing"] = ("wall time of rijk_scf, the fastest of %d runs (ms_inside: the library's own clock of "
                          "that run, without argument checks and buffer release; ms_setup: before the first "
                          "iteration, uploads, overlap eigendecomposition and the guess's build and diagonalisation; "
-                         "ms_final: after the last iteration, closing build and orbitals)")
+                         "ms_final: after the last iteration, closing build and orbitals)" % reps)
         scf = out
+    fb.close()
+    del dD, dMO, dJ, dK
+    torch.cuda.empty_cache()
 
-    cpu = {"skipped": cpu_skip} if cpu_skip else None
+    cpu = None
     if want_cpu:
-        v, threads, sample = cpu_builds_per_s(si, DM, MO, args.cpu_seconds)
-        cpu = {"value": v, "unit": "builds/s", "cores": threads, "kind": "port", "sample": sample}
+        cpu = cpu_baseline_for(si, DM, MO, args.workload, args.seed, args.cpu_slices, args.cpu_seconds)
+
+    extra = scf_small = None
+    if rank == 0 and world == 1 and not synthetic and args.extra not in ("none", "", args.workload):
+        extra = extra_workload(args.extra, args.seed, dev, max(5, args.steps // 2), want_cpu, args.cpu_seconds / 2)
+        if want_cpu and not args.no_scf:
+            scf_small = scf_cpu_small(args.seed, dev)
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
                "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
                "scaling": "strong" if sharded else "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": WORKLOAD_NAMES.get(args.workload, args.workload if not synthetic else
-                                                        "synthetic " + args.workload[5:].replace(",", " ") +
-                                                        " (random packed B ~ N(0,1) e^-|mu-nu|/n)"),
-                          "n": n, "naux": naux, "nocc": nocc,
-                          "parallelism": ("aux-sharded x%d" % world) if sharded else
-                                         ("replicas x%d" % world if world > 1 else "single"),
-                          "l2": "inputs larger than L2 (B = %.2f GB)" % (st0["bytes_b"] / 1e9),
-                          "seed": args.seed},
+               "config": config_of(args.workload, n, naux, nocc, world, sharded, args.seed),
                "e2e": {"value": (1 if sharded else world) * 1e3 / ms_e2e, "unit": "builds/s",
-                       "h2d_bytes_per_step": int((n * n + nocc * n) * 8), "d2h_bytes_per_step": int(2 * n * n * 8)},
+                       "h2d_bytes_per_step": int((n * n + nocc * n) * 8), "d2h_bytes_per_step": int(2 * n * n * 8),
+                       "host_buffers": "pinned"},
+               "e2e_pageable": {"value": (1 if sharded else world) * 1e3 / ms_e2e_pg, "unit": "builds/s",
+                                "steps": psteps, "host_buffers": "pageable numpy arrays"},
                "gpu_launches": launches,
                "roofline": roof, "coulomb_roofline": coul, "stage_ms": stage_ms,
                "mixed": mixed, "fp64_tc": fp64tc, "scf": scf, "cpu_baseline": cpu, "clocks": clk.summary(),
@@ -617,8 +828,13 @@ def main():
                          "gpu_integrals_ms": st0["ms_setup_ints"] if args.setup == "gpu" else None,
                          "metric_ms": st0["ms_setup_metric"], "b_ms": st0["ms_setup_3c"],
                          "host_integrals_s": tint, "host_ri_integrals": need_host_ri}}
+        if cpu and "value" in cpu:
+            out["ratio_vs_cpu"] = {"value": value / cpu["value"], "e2e": out["e2e"]["value"] / cpu["value"]}
+        if extra is not None:
+            out["extra_" + args.extra] = extra
+        if scf_small is not None:
+            out["scf_cpu_vs_gpu_h2o6"] = scf_small
         print(json.dumps(out), flush=True)
-    fb.close()
     if dist is not None:
         dist.destroy_process_group()
 

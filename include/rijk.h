@@ -155,6 +155,13 @@ int rijk_fock_device(rijk_ctx* ctx, const double* dDM, const double* dMO, long n
  * a bounded device-side wait ran out); also refreshes the timing statistics. */
 int rijk_sync(rijk_ctx* ctx);
 
+/* Self-test of the bounded-wait error path (no reference counterpart).  Launches one warp on the
+ * context's stream that allocates TMEM as the tcgen05 kernels do, waits on an mbarrier nothing ever
+ * arrives on until `cycles` SM clock cycles (1000 .. 2e9) have passed, then raises the timeout bit,
+ * frees the TMEM and returns.  Asynchronous; the next rijk_sync returns RIJK_ERR_TIMEOUT, and the
+ * context stays usable. */
+int rijk_selftest_wait_timeout(rijk_ctx* ctx, long long cycles);
+
 /* Size of the fixed device scratch used by rijk_coulomb_noalloc (per GPU, held until exit). */
 #define RIJK_NOALLOC_SCRATCH_BYTES (32L * 1024 * 1024)
 
@@ -168,8 +175,9 @@ int rijk_sync(rijk_ctx* ctx);
  * RIJK_NOALLOC_SCRATCH_BYTES device array inside the library:
  *  - sizes that need more return RIJK_ERR_ARG (about n_ao <= 1980 fits);
  *  - all calls on one GPU share it, so calls that overlap on the GPU race;
- *  - the first call on each device looks up the array's address and should come before any
- *    stream capture.
+ *  - rijk_create looks up the array's address on its device, which is when the array is
+ *    allocated there (so create the context before handing the GPU's memory to a pool).
+ * After rijk_set_aux_range the result is that slice's partial J, as with rijk_fock_device.
  * The call makes no cudaMalloc, cudaFree or allocating library call. */
 int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ);
 

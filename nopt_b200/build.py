@@ -32,6 +32,7 @@ CUDA_SOURCES = [
     "rijk/k_eri.cu",
     "rijk/k_mo_ri.cu",
     "rijk/rijk_cache.cu",
+    "rijk/rijk_selftest.cu",
 ]
 
 
@@ -60,20 +61,35 @@ def build_host(force=False):
     return out
 
 
+def _headers():
+    out = []
+    for d in (INC, os.path.join(CSRC, "rijk"), os.path.join(CSRC, "host")):
+        if os.path.isdir(d):
+            out += [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".h", ".cuh"))]
+    return out
+
+
 def build_cuda(force=False, extra=()):
+    """Compiles each stale object (older than its source or any header) in parallel, then links."""
+    from concurrent.futures import ThreadPoolExecutor
     out = os.path.join(HERE, "librijk.so")
     srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES if os.path.exists(os.path.join(CSRC, s))]
-    if force or _stale(out, srcs):
-        objdir = os.path.join(HERE, "_build")
-        os.makedirs(objdir, exist_ok=True)
-        objs = []
-        for s in srcs:
-            o = os.path.join(objdir, os.path.basename(s) + ".o")
-            _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-                                  "-I" + INC, "-I" + os.path.join(CSRC, "rijk"), "-I" + os.path.join(CSRC, "host"),
-                                  "--expt-relaxed-constexpr",
-                                  "-c", s, "-o", o] + list(extra))
-            objs.append(o)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    hdr_t = max([os.path.getmtime(h) for h in _headers()] or [0.0])
+    jobs, objs = [], []
+    for s in srcs:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        objs.append(o)
+        if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t):
+            jobs.append([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                                         "-Xcompiler", "-fvisibility=hidden", "-I" + INC,
+                                         "-I" + os.path.join(CSRC, "rijk"), "-I" + os.path.join(CSRC, "host"),
+                                         "--expt-relaxed-constexpr", "-c", s, "-o", o] + list(extra))
+    if jobs:
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
+            list(ex.map(_run, jobs))
+    if jobs or not os.path.exists(out) or os.path.getmtime(out) < max(os.path.getmtime(o) for o in objs):
         _run([NVCC] + ARCH + ["-shared", "-o", out] + objs + ["-lcusolver", "-lcublas", "-lcudart"])
     return out
 

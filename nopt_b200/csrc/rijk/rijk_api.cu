@@ -279,6 +279,10 @@ RIJK_API int rijk_create(rijk_ctx** out, int device) {
   }
   cublasSetStream(ctx->cublas, ctx->stream);
   cusolverDnSetStream(ctx->cusolver, ctx->stream);
+  if (int rc = rijk::noalloc_resolve(ctx)) {
+    rijk_destroy(ctx);
+    return rc;
+  }
   if (ensure(ctx, ctx->err, sizeof(int), "err")) {
     rijk_destroy(ctx);
     return RIJK_ERR_ALLOC;

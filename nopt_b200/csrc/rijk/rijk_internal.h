@@ -79,6 +79,7 @@ struct rijk_ctx {
                             // blocks of 8 digits x 32 bytes
   rijk::DeviceBuf Xe;       // their row exponents, parts x npad2
   rijk::DeviceBuf scf[32];  // rijk_scf's work buffers, kept between calls
+  double* noalloc_scratch = nullptr;  // device address of rijk_coulomb_noalloc's fixed scratch on `device`
 
   rijk_stats_t stats{};
   std::string last_error;
@@ -120,6 +121,12 @@ int set_metric_impl(rijk_ctx* ctx, const double* PQ, cudaMemcpyKind kind, long n
 // naux) into the device buffer raw.
 using ChunkFill = std::function<int(long mu0, long mu1, long first, long count, double* raw, long ld)>;
 int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& fill);
+
+// ---- rijk_noalloc.cu
+// Looks up the device address of rijk_coulomb_noalloc's fixed scratch array on ctx->device (which
+// must be current) into ctx->noalloc_scratch.  The lookup loads the module holding the array, and
+// with it the array itself, so rijk_create does it while allocating is still allowed.
+int noalloc_resolve(rijk_ctx* ctx);
 
 // ---- k_pack.cu
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);

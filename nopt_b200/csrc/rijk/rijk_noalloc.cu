@@ -18,12 +18,12 @@
 //  - makes two calls that overlap on one GPU (on different streams) race.
 //
 // Host code cannot pass the array's name to a kernel: on the host it is only a stand-in, not a
-// device address. The first call on each device therefore looks the address up with
-// cudaGetSymbolAddress (with that device current) and caches it. That first call should come
-// before any stream capture.
+// device address.  rijk_create looks the address up with cudaGetSymbolAddress (with the context's
+// device current) and keeps it in the context.  With CUDA's lazy module loading that lookup is what
+// loads this file's module and allocates the array on the device, so it happens at set-up, while
+// allocating is still allowed, and never inside rijk_coulomb_noalloc.  A context created after a
+// device reset looks the address up again.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "gemm_f64.cuh"
 #include "rijk_internal.h"
@@ -35,38 +35,26 @@ static constexpr long kNoallocScratchDoubles = RIJK_NOALLOC_SCRATCH_BYTES / stat
 static __device__ __align__(256) double g_rijk_noalloc_scratch[kNoallocScratchDoubles];
 
 namespace rijk {
-int set_err(rijk_ctx* ctx, int code, const char* fmt, ...);
-int cuda_check(rijk_ctx* ctx, cudaError_t e, const char* what);
-}  // namespace rijk
 
-namespace {
-
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-double* g_scratch_dev[kMaxDevices] = {};
-
-// Device address of the scratch array on `device` (the caller has made it current).
-int scratch_address(rijk_ctx* ctx, int device, double** out) {
-  if (device < 0 || device >= kMaxDevices)
-    return rijk::set_err(ctx, RIJK_ERR_ARG, "rijk_coulomb_noalloc: device ordinal %d out of range", device);
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_dev[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_rijk_noalloc_scratch);
-    if (e != cudaSuccess) return rijk::cuda_check(ctx, e, "rijk_coulomb_noalloc: cudaGetSymbolAddress");
-    g_scratch_dev[device] = static_cast<double*>(p);
+int noalloc_resolve(rijk_ctx* ctx) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_rijk_noalloc_scratch);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? RIJK_ERR_ALLOC : RIJK_ERR_CUDA;
   }
-  *out = g_scratch_dev[device];
+  ctx->noalloc_scratch = static_cast<double*>(p);
   return RIJK_OK;
 }
 
-}  // namespace
+}  // namespace rijk
 
 RIJK_API int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ) {
   using namespace rijk;
   if (!ctx) return RIJK_ERR_ARG;
   if (!dDM || !dJ) return set_err(ctx, RIJK_ERR_ARG, "rijk_coulomb_noalloc: null pointer");
   if (!ctx->have_b) return set_err(ctx, RIJK_ERR_STATE, "rijk_coulomb_noalloc before rijk_set_3c");
+  if (!ctx->noalloc_scratch) return set_err(ctx, RIJK_ERR_STATE, "rijk_coulomb_noalloc: no scratch address");
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_check(ctx, e, "rijk_coulomb_noalloc: cudaSetDevice");
 
@@ -84,11 +72,8 @@ RIJK_API int rijk_coulomb_noalloc(rijk_ctx* ctx, const double* dDM, double* dJ) 
   const long fit = (kNoallocScratchDoubles - tile_elems - nauxr) / tile_elems;
   if (nsplit > fit) nsplit = static_cast<int>(fit);
 
-  double* scratch = nullptr;
-  int rc = scratch_address(ctx, ctx->device, &scratch);
-  if (rc) return rc;
-  double* Dt = scratch;
-  double* w = scratch + tile_elems;
+  double* Dt = ctx->noalloc_scratch;
+  double* w = Dt + tile_elems;
   double* Jpart = w + nauxr;
 
   cudaStream_t s = ctx->stream;

@@ -49,16 +49,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Wait for the phase with the given parity; gives up after kWaitCycles or when another role
-// has raised *abort.  Returns false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+// Wait for the phase with the given parity; gives up after `limit` SM clock cycles or when another
+// role has raised *abort.  Returns false when it gave up.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, volatile int* abort, long long limit) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort) return false;
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   }
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  return mbar_wait_for(bar, parity, abort, kWaitCycles);
 }
 
 // 2-D TMA tile load global -> shared, completion signalled on `bar` (transaction bytes).

@@ -136,6 +136,30 @@ def coulomb_3c(orb, aux, layout=LAYOUT_PACKED):
     return out
 
 
+def aux_slice_bounds(aux, nslices):
+    """About nslices ranges [(p0, p1), ...] of aux functions covering [0, nbf), cut at shell
+    boundaries (each range is then one sub-basis of whole shells)."""
+    offs = list(aux.shell_offsets()) + [aux.nbf]
+    target = aux.nbf / max(int(nslices), 1)
+    bounds, p0 = [], 0
+    for s in range(1, len(offs)):
+        if offs[s] - p0 >= target or s == len(offs) - 1:
+            if offs[s] > p0:
+                bounds.append((p0, int(offs[s])))
+                p0 = int(offs[s])
+    return bounds
+
+
+def coulomb_3c_aux_range(orb, aux, p0, p1, layout=LAYOUT_NOPT_FULL):
+    """(mu nu|P) for the aux functions [p0, p1), which must start and end on shell boundaries:
+    the three-centre integrals of the sub-basis of those shells, (n^2 or n(n+1)/2) x (p1 - p0)."""
+    offs = list(aux.shell_offsets()) + [aux.nbf]
+    if p0 not in offs or p1 not in offs or p1 <= p0:
+        raise ValueError("aux range [%d, %d) does not fall on shell boundaries" % (p0, p1))
+    sub = Basis(aux.shells[offs.index(p0):offs.index(p1)], pure=aux.pure)
+    return coulomb_3c(orb, sub, layout)
+
+
 def atomic_density(sym, orb_basis, aux_basis):
     """(D, rows) of one atom of element `sym` at the origin (see gto_atomic_density)."""
     from .molecules import Z_OF

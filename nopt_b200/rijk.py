@@ -119,6 +119,8 @@ def lib():
         L.rijk_fock.argtypes = [_vp, _dp, _dp, ctypes.c_long, _dp, _dp, ctypes.c_int]
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
+        L.rijk_selftest_wait_timeout.argtypes = [_vp, ctypes.c_longlong]
+        L.rijk_coulomb_noalloc.argtypes = [_vp, _vp, _vp]
         L.rijk_grad.argtypes = [_vp, _dp, ctypes.c_long, _dp, ctypes.c_double, _dp, _dp, _dp, _dp]
         L.rijk_mo_ints.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
         L.rijk_scf.argtypes = [_vp, _dp, _dp, ctypes.c_long, ctypes.c_double, P(ScfOpts), _dp, P(ScfResult)]
@@ -338,6 +340,11 @@ class FockBuilder:
 
     def sync(self):
         self._check(lib().rijk_sync(self._h))
+
+    def selftest_wait_timeout(self, cycles):
+        """Launch the bounded-wait self-test (a wait that runs out after `cycles` SM clocks); the
+        next sync raises RijkError with ERR_TIMEOUT."""
+        self._check(lib().rijk_selftest_wait_timeout(self._h, int(cycles)))
 
     def calc_f_ao(self, H, DM, J, K, c=1.0, mc=0, e_nuc=0.0):
         n = self.n

@@ -76,6 +76,49 @@ def dm_to_f_transform_ri(RI_AA, Vm05, DM, MO, n_c, n_ao):
     return J, K
 
 
+# --------------------------------------------------- aux-sliced restatement ------
+# DM_to_F_transform_RI (src/RI.cpp:115-176) with the raw three-centre tensor held one slice of aux
+# functions at a time, for sizes whose full-square RI_AA (n^2 naux doubles) exceeds host memory.
+# The reference's stages and their order are kept; each is cut along the aux index:
+#   set-up (once per density):  RI_J = vec(D)^T RI_AA and RI_CA = MO RI_AA, slice by slice
+#                               (:122-126, :146-150), then RI_J <- V^-1/2 V^-1/2 RI_J (:128-138);
+#   one slice [p0, p1):         the slice's RI_J and RI_CA columns again (the same products),
+#                               RI_CA2 columns Q in the slice = RI_CA V^-1/2[:, Q] (:152-156),
+#                               their transpose (:158-164), K_s = T T^T (:167-171) and
+#                               J_s = RI_AA[:, slice] RI_J[slice] (:140-144).
+# Every product of a full build belongs to exactly one slice, so a slice carries (p1 - p0) / naux
+# of the build's arithmetic, and J = sum_s J_s, K = sum_s K_s over slices that cover [0, naux).
+
+def sliced_setup(raw_slice, bounds, Vm05, DM, MO, n_c, n_ao):
+    """RI_CA (n_c, n_ao, naux) and the fitted Coulomb coefficients V^-1/2 V^-1/2 RI_J from every
+    slice.  raw_slice(p0, p1) returns RI_AA[:, p0:p1] as an (n_ao^2, p1 - p0) array."""
+    naux = Vm05.shape[0]
+    MOc = np.ascontiguousarray(MO[:n_c])
+    RI_CA = np.empty((n_c, n_ao, naux))
+    RI_J = np.empty(naux)
+    for p0, p1 in bounds:
+        A = raw_slice(p0, p1)
+        RI_J[p0:p1] = DM.reshape(1, n_ao * n_ao) @ A                              # :122-126
+        RI_CA[:, :, p0:p1] = (MOc @ A.reshape(n_ao, n_ao * (p1 - p0))).reshape(n_c, n_ao, p1 - p0)  # :146-150
+    RI_Jv = Vm05 @ (Vm05 @ RI_J)                                                  # :128-138
+    return RI_CA, RI_Jv
+
+
+def sliced_step(A, p0, p1, RI_CA, RI_Jv, Vm05, DM, MO, n_c, n_ao):
+    """The share of aux slice [p0, p1) of one build; A = RI_AA[:, p0:p1].  Returns (J_s, K_s):
+    J_s sums the raw aux functions P of the slice, K_s the fitted aux functions Q of the slice."""
+    s = p1 - p0
+    naux = Vm05.shape[0]
+    MOc = np.ascontiguousarray(MO[:n_c])
+    RI_J = DM.reshape(1, n_ao * n_ao) @ A                                         # :122-126
+    RI_CA[:, :, p0:p1] = (MOc @ A.reshape(n_ao, n_ao * s)).reshape(n_c, n_ao, s)  # :146-150
+    RI_CA2 = RI_CA.reshape(n_c * n_ao, naux) @ Vm05[:, p0:p1]                     # :152-156
+    T = RI_CA2.reshape(n_c, n_ao, s).transpose(1, 0, 2).reshape(n_ao, n_c * s)    # :158-164
+    K = T @ T.T                                                                   # :167-171
+    J = (A @ RI_Jv[p0:p1]).reshape(n_ao, n_ao)                                    # :140-144
+    return J, K, RI_J
+
+
 def calc_2el_mo_ints_ri(RI_AA, Vm05, n_ao, DM_D, MO_VEC, MO_VEC1, MO_VEC2, n_c, n_a, t=0):
     """calc_2el_MO_INTS_RI (src/RI.cpp:178-292): active integrals MO_INTS (n_a^2 x n_a^2) in the
     reference's (b a | d c) order, then the core J, K of DM_D / MO_VEC (None when DM_D is None)."""
