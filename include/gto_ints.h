@@ -65,6 +65,12 @@ int gto_coulomb_3c(const gto_basis* orb, const gto_basis* aux, int layout, doubl
 int gto_atomic_density(const gto_basis* orb, const gto_basis* aux, double Z, const double* xyz, double* D,
                        double* rows, int* nrows);
 
+/* The (2l+1) x ncart(l) row-major matrix C of the spherical functions of angular momentum l (0 .. 4)
+ * in terms of the Cartesian ones of the same shell, Y_m = sum_c C[m][c] phi_c, with both normalised
+ * as in the integrals (the map a Cartesian orbital basis is projected with, as the reference's
+ * T_D5, src/molecule.cpp:4551-4680). */
+int gto_cart_to_sph(int l, double* out);
+
 /* Boys function F_m(T), m = 0..mmax (test hook). */
 int gto_boys(int mmax, double T, double* F);
 

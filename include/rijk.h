@@ -220,6 +220,15 @@ typedef struct {
   int fp64_phase_precision; /* 0 (default): RIJK_PREC_FP64 builds after a mixed phase (and for a
                              closing build); RIJK_PREC_FP64_TC: the same FP64-accurate results
                              with K on the int8 tensor cores                                    */
+  /* Optional orbital-space projector (appended fields; NULL = the whole AO space): an n_ao x
+   * n_proj row-major host array T whose columns span the space the orbitals are confined to, as
+   * the reference's Cartesian->spherical T_D5 (n_ao x n_ao_d5, make_D5_matr, src/molecule.cpp:4551-
+   * 4680).  The orthogonaliser then comes from T^T S T (eigenvalues below lindep dropped), so every
+   * diagonalisation runs in the projected space as diag_X_AO_in_MO does with D5 = 1
+   * (src/molecule.cpp:4004-4050), while the Fock builds stay in the n_ao Cartesian AO basis.  MO
+   * receives n_proj (less dropped) orbitals as rows of n_ao coefficients, the rest zero.        */
+  const double* ao_projector;
+  long n_proj;            /* 1 .. n_ao                                                          */
 } rijk_scf_opts_t;
 
 #define RIJK_CONV_DIIS 0

@@ -33,6 +33,7 @@ CUDA_SOURCES = [
     "rijk/k_mo_ri.cu",
     "rijk/rijk_cache.cu",
     "rijk/rijk_selftest.cu",
+    "rijk/k_gemm.cu",
 ]
 
 

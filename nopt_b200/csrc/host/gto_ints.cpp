@@ -320,6 +320,13 @@ int gto_basis_shell_offsets(const gto_basis* b, int* out) {
   return GTO_OK;
 }
 
+int gto_cart_to_sph(int l, double* out) {
+  if (l < 0 || l > LMAX || !out) return GTO_ERR_ARG;
+  const std::vector<double>& c = gto_tab::sph().c[l];
+  std::copy(c.begin(), c.end(), out);
+  return GTO_OK;
+}
+
 int gto_boys(int mmax, double T, double* F) {
   if (mmax < 0 || mmax > LTOT || T < 0.0 || !F) return GTO_ERR_ARG;
   std::call_once(g_boys_once, boys_table_init);

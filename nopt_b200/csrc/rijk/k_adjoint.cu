@@ -14,13 +14,14 @@
 //     dE/d(P|Q)    = -(M^T G M)_PQ,  G_QR = (1/2) sum_{mu nu} Gamma^Q_{mu nu} B^R_{mu nu}
 // (E depends on the metric only through V^-1 = M^T M, for either metric form).
 //
-// Device work, FP64 throughout: one FP64 Fock build (which leaves w and the half-transformed
-// XT in the context), then, over chunks of aux functions, the small products Y^Q = X^Q C^T and
-// T^Q = Y^Q C (cuBLAS strided-batched DGEMM), k_gamma_f64 forming the packed Gamma tiles
-// Gamma^Q_tile = 4 w_Q D_tile - 2 T^Q_rows Ct_cols^T with DMMA, and two DGEMMs contracting the
-// chunk of Gamma with M (raw three-centre gradient, accumulated) and with B (its rows of G, the
-// metric gradient).  When HBM cannot hold Gamma for every aux function at once, each chunk's
-// X^Q is recomputed in tiles from B instead of read from the stored tensor.
+// Device work, FP64 throughout, every contraction on hand-written DMMA kernels: one FP64 Fock build
+// (which leaves w and the half-transformed XT in the context), then, over chunks of aux functions,
+// the small batched products Y^Q = X^Q C^T and T^Q = Y^Q C (k_gemm_f64), k_gamma_f64 forming the
+// packed Gamma tiles Gamma^Q_tile = 4 w_Q D_tile - 2 T^Q_rows Ct_cols^T, and two contractions of
+// the chunk of Gamma: with M, written straight into the packed pair layout of dE/d(P|mu nu)
+// (accumulated over chunks), and with B, the chunk's rows of G (diagonal tiles weighted 1/2).  When
+// HBM cannot hold Gamma for every aux function at once, each chunk's X^Q is recomputed in tiles
+// from B instead of read from the stored tensor.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -107,34 +108,6 @@ __global__ void k_transpose_mo(const double* __restrict__ MOp, long noccp, long 
   }
 }
 
-// Scale Gamma in place by the packed-storage weight of its tile (2 off the diagonal, 1 on it).
-__global__ void k_scale_offdiag(double* __restrict__ G, long naux, long ntile, double f_off, double f_diag) {
-  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const long total = naux * ntile * TILE2;
-  for (; idx < total; idx += static_cast<long>(gridDim.x) * blockDim.x) {
-    long t = (idx / TILE2) % ntile;
-    long I, J;
-    tri_decode(t, I, J);
-    G[idx] *= (I == J) ? f_diag : f_off;
-  }
-}
-
-// dI3[(mu(mu+1)/2 + nu) * naux + P] = f(mu, nu) * R[e(mu, nu) + P * te], R column-major (te x naux)
-__global__ void k_gather_pairs(const double* __restrict__ R, long te, long n, long naux, double* __restrict__ out) {
-  const long npair = n * (n + 1) / 2;
-  long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  for (; idx < npair * naux; idx += static_cast<long>(gridDim.x) * blockDim.x) {
-    long pr = idx / naux, P = idx % naux;
-    long mu = static_cast<long>((sqrt(8.0 * static_cast<double>(pr) + 1.0) - 1.0) * 0.5);
-    while (mu * (mu + 1) / 2 > pr) --mu;
-    while ((mu + 1) * (mu + 2) / 2 <= pr) ++mu;
-    long nu = pr - mu * (mu + 1) / 2;
-    long I = mu / TILE, J = nu / TILE;
-    long e = tri_index(I, J) * TILE2 + (mu % TILE) * TILE + (nu % TILE);
-    out[idx] = (mu == nu ? 1.0 : 2.0) * R[e + P * te];
-  }
-}
-
 __global__ void k_fock_sym(const double* __restrict__ H, const double* __restrict__ J, const double* __restrict__ K,
                            long nn, double* __restrict__ F) {
   long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -194,15 +167,12 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
     return set_err(ctx, RIJK_ERR_STATE, "rijk_grad needs all aux functions in one context (no aux range)");
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
-  cublasHandle_t cb = ctx->cublas;
   const long n = ctx->n, naux = ctx->naux, npad = ctx->npad, nt = ctx->nt, ntile = ctx->ntile;
   const long nn = n * n, te = ntile * TILE2, noccp = round_up(nocc, 16), nauxp = round_up(naux, KC);
-  const int ni = static_cast<int>(n), nci = static_cast<int>(nocc);
-  const double one = 1.0, zero = 0.0;
   const size_t b_nn = nn * sizeof(double);
-  DeviceBuf dMO, dH, dD, dJ, dK, dF, dG, red, Y, Tb, Ct, Gam, R, Gm, T1, out;
+  DeviceBuf dMO, dH, dD, dJ, dK, dF, dG, red, Y, Tb, Ct, Gam, Gm, T1, out;
   auto cleanup = [&]() {
-    DeviceBuf* all[] = {&dMO, &dH, &dD, &dJ, &dK, &dF, &dG, &red, &Y, &Tb, &Ct, &Gam, &R, &Gm, &T1, &out};
+    DeviceBuf* all[] = {&dMO, &dH, &dD, &dJ, &dK, &dF, &dG, &red, &Y, &Tb, &Ct, &Gam, &Gm, &T1, &out};
     for (DeviceBuf* b : all) release(*b);
   };
   auto chk = [&](int r) {
@@ -220,17 +190,29 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   double* pF = static_cast<double*>(dF.p);
   cudaMemcpyAsync(pMO, MO, nocc * n * sizeof(double), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(dH.p, H, b_nn, cudaMemcpyHostToDevice, s);
-  // D = C^T C: MO row-major (n_c x n) is column-major (n x n_c)
-  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, ni, ni, nci, &one, pMO, ni, pMO, ni, &zero, pD, ni);
+  {  // D[mu][nu] = sum_i C[i][mu] C[i][nu]
+    GemmF64Args g;
+    g.M = n, g.N = n, g.K = nocc;
+    g.A = pMO, g.lda = n, g.a_kmajor = false;
+    g.B = pMO, g.ldb = n, g.b_kmajor = false;
+    g.C = pD, g.ldc = n;
+    gemm_f64(g, 1, s);
+  }
   if ((rc = chk(fock_device_impl(ctx, pD, pMO, nocc, static_cast<double*>(dJ.p), static_cast<double*>(dK.p),
                                  RIJK_PREC_FP64))))
     return rc;
   k_fock_sym<<<grid_of(nn), 256, 0, s>>>(static_cast<const double*>(dH.p), static_cast<const double*>(dJ.p),
                                          static_cast<const double*>(dK.p), nn, pF);
   k_energy_partial<<<512, 256, 0, s>>>(pD, pF, static_cast<const double*>(dH.p), nn, static_cast<double*>(red.p));
-  // dE/dC = 4 C F  (column-major n x n_c = 4 F Mt)
-  const double four = 4.0;
-  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, ni, nci, ni, &four, pF, ni, pMO, ni, &zero, static_cast<double*>(dG.p), ni);
+  {  // dE/dC[i][mu] = 4 sum_nu C[i][nu] F[nu][mu]
+    GemmF64Args g;
+    g.M = nocc, g.N = n, g.K = n;
+    g.A = pMO, g.lda = n, g.a_kmajor = true;
+    g.B = pF, g.ldb = n, g.b_kmajor = false;
+    g.C = static_cast<double*>(dG.p), g.ldc = n;
+    g.alpha = 4.0;
+    gemm_f64(g, 1, s);
+  }
   std::vector<double> part(1024);
   cudaMemcpyAsync(part.data(), red.p, 1024 * sizeof(double), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(dEdC, dG.p, nocc * n * sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -252,12 +234,10 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   // chunk size set by rijk_set_grad_chunk) each chunk's X^Q is recomputed in tiles by the
   // half-transform kernel, and only one chunk of X, Y, T and Gamma exists at a time.
   const long kdim = naux * noccp;
+  const long npair = n * (n + 1) / 2;
   const double* MOp = static_cast<const double*>(ctx->MOp.p);
   const double* pM = static_cast<const double*>(ctx->M.p);  // row-major [Q][P], ld nauxp
-  const int na = static_cast<int>(naux), nap = static_cast<int>(nauxp), tei = static_cast<int>(te);
-  const int ncp = static_cast<int>(noccp), npi = static_cast<int>(npad);
-  if (dEdI3 && ((rc = chk(ensure(ctx, R, static_cast<size_t>(te) * naux * sizeof(double), "grad R"))) ||
-                (rc = chk(ensure(ctx, out, static_cast<size_t>(n * (n + 1) / 2) * naux * sizeof(double), "grad dI3")))))
+  if (dEdI3 && (rc = chk(ensure(ctx, out, static_cast<size_t>(npair) * naux * sizeof(double), "grad dI3"))))
     return rc;
   if (dEdPQ && ((rc = chk(ensure(ctx, Gm, static_cast<size_t>(naux) * naux * sizeof(double), "grad G"))) ||
                 (rc = chk(ensure(ctx, T1, static_cast<size_t>(naux) * naux * sizeof(double), "grad T1")))))
@@ -284,12 +264,12 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
     return rc;
   }
   double* pGam = static_cast<double*>(Gam.p);
+  double* pY = static_cast<double*>(Y.p);
+  double* pT = static_cast<double*>(Tb.p);
   const size_t gsmem = 4 * 64 * LDK * sizeof(double);
   ensure_smem_limit(reinterpret_cast<const void*>(k_gamma_f64), gsmem);
-  const double half = 0.5;
   for (long q0 = 0; q0 < naux; q0 += qc) {
     const long nq = std::min(qc, naux - q0);
-    const int nqi = static_cast<int>(nq);
     const double* X;  // X^Q_{i nu} at X[nu * ldx + (Q - q0) * noccp + i]
     long ldx;
     if (recompute) {
@@ -300,44 +280,69 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
       X = static_cast<const double*>(ctx->XT.p) + q0 * noccp;
       ldx = kdim;
     }
-    // Y^Q (noccp x noccp) = X^Q (noccp x npad, column-major view, ld ldx) . Cm (npad x noccp)
-    cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, ncp, ncp, npi, &one, X, static_cast<int>(ldx), noccp, MOp,
-                              npi, 0, &zero, static_cast<double*>(Y.p), ncp, noccp * noccp, nqi);
-    // T^Q as [mu][i] = (Y^Q C) column-major (noccp x npad): Y^Q (noccp x noccp) . Cm^T
-    cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_T, ncp, npi, ncp, &one, static_cast<const double*>(Y.p), ncp,
-                              noccp * noccp, MOp, npi, 0, &zero, static_cast<double*>(Tb.p), ncp, npad * noccp, nqi);
+    {  // Y^Q[i][j] = sum_nu X^Q_{i nu} C_{j nu}   (= C B^Q C^T)
+      GemmF64Args g;
+      g.M = noccp, g.N = noccp, g.K = npad;
+      g.A = X, g.lda = ldx, g.sA = noccp, g.a_kmajor = false;
+      g.B = MOp, g.ldb = npad, g.sB = 0, g.b_kmajor = true;
+      g.C = pY, g.ldc = noccp, g.sC = noccp * noccp;
+      gemm_f64(g, nq, s);
+    }
+    {  // T^Q[mu][i] = sum_j C_{j mu} Y^Q[j][i]
+      GemmF64Args g;
+      g.M = npad, g.N = noccp, g.K = noccp;
+      g.A = MOp, g.lda = npad, g.sA = 0, g.a_kmajor = false;
+      g.B = pY, g.ldb = noccp, g.sB = noccp * noccp, g.b_kmajor = false;
+      g.C = pT, g.ldc = noccp, g.sC = npad * noccp;
+      gemm_f64(g, nq, s);
+    }
     dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(nq));
-    k_gamma_f64<<<grid, G_THREADS, gsmem, s>>>(static_cast<const double*>(Tb.p), static_cast<const double*>(Ct.p), pD,
+    k_gamma_f64<<<grid, G_THREADS, gsmem, s>>>(pT, static_cast<const double*>(Ct.p), pD,
                                                static_cast<const double*>(ctx->w.p) + q0, n, npad, noccp, te, pGam);
     if (dEdI3) {
-      // R (te x naux, column-major) += Gamma_chunk_cm (te x nq) . (rows q0.. of M, as nq x naux)
-      const double beta = q0 == 0 ? 0.0 : 1.0;
-      cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, tei, na, nqi, &one, pGam, tei, pM + q0 * nauxp, nap, &beta,
-                  static_cast<double*>(R.p), tei);
+      // dE/d(P|mu nu) += sum_{Q in chunk} Gamma^Q_{mu nu} M_QP, straight into the packed pair rows
+      GemmF64Args g;
+      g.M = te, g.N = naux, g.K = nq;
+      g.A = pGam, g.lda = te, g.a_kmajor = false;
+      g.B = pM + q0 * nauxp, g.ldb = nauxp, g.b_kmajor = false;
+      g.C = static_cast<double*>(out.p), g.ldc = naux;
+      g.beta = q0 == 0 ? 0.0 : 1.0;
+      g.mode = GEMM_PAIRS;
+      g.n_ao = n;
+      gemm_f64(g, 1, s);
     }
     if (dEdPQ) {
-      // rows q0.. of G = 1/2 sum_e omega_e Gamma[Q][e] B[R][e] (omega = 2 off-diagonal tiles)
-      k_scale_offdiag<<<grid_of(nq * te), 256, 0, s>>>(pGam, nq, ntile, 2.0, 1.0);
-      cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nqi, na, tei, &half, pGam, tei, static_cast<const double*>(ctx->B.p),
-                  tei, &zero, static_cast<double*>(Gm.p) + q0, na);
+      // rows q0.. of G_QR = 1/2 sum_{mu nu} Gamma^Q B^R over the full squares: each stored element
+      // of an off-diagonal tile once, of a diagonal tile one half
+      GemmF64Args g;
+      g.M = nq, g.N = naux, g.K = te;
+      g.A = pGam, g.lda = te, g.a_kmajor = true;
+      g.B = static_cast<const double*>(ctx->B.p), g.ldb = te, g.b_kmajor = true;
+      g.C = static_cast<double*>(Gm.p) + q0 * naux, g.ldc = naux;
+      g.kdiag = 1;
+      gemm_f64(g, 1, s);
     }
   }
   release(Xc);
   release(Y);
   release(Tb);
-  if (dEdI3) {
-    k_gather_pairs<<<grid_of(n * (n + 1) / 2 * naux), 256, 0, s>>>(static_cast<const double*>(R.p), te, n, naux,
-                                                                   static_cast<double*>(out.p));
-    cudaMemcpyAsync(dEdI3, out.p, static_cast<size_t>(n * (n + 1) / 2) * naux * sizeof(double),
-                    cudaMemcpyDeviceToHost, s);
-  }
+  if (dEdI3)
+    cudaMemcpyAsync(dEdI3, out.p, static_cast<size_t>(npair) * naux * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (dEdPQ) {
-    // dE/dV = -M^T G M:  T1 = G M_cm^T ; dEdPQ = -M_cm T1  (M_cm = M^T as a column-major naux x naux block, ld nauxp)
-    const double mone = -1.0;
-    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, na, na, na, &one, static_cast<const double*>(Gm.p), na, pM, nap, &zero,
-                static_cast<double*>(T1.p), na);
-    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, na, na, na, &mone, pM, nap, static_cast<const double*>(T1.p), na, &zero,
-                static_cast<double*>(Gm.p), na);
+    // dE/dV = -M^T G M:  T1[Q][P'] = sum_R G[Q][R] M[R][P'];  out[P][P'] = -sum_Q M[Q][P] T1[Q][P']
+    GemmF64Args g;
+    g.M = naux, g.N = naux, g.K = naux;
+    g.A = static_cast<const double*>(Gm.p), g.lda = naux, g.a_kmajor = true;
+    g.B = pM, g.ldb = nauxp, g.b_kmajor = false;
+    g.C = static_cast<double*>(T1.p), g.ldc = naux;
+    gemm_f64(g, 1, s);
+    GemmF64Args h;
+    h.M = naux, h.N = naux, h.K = naux;
+    h.A = pM, h.lda = nauxp, h.a_kmajor = false;
+    h.B = static_cast<const double*>(T1.p), h.ldb = naux, h.b_kmajor = false;
+    h.C = static_cast<double*>(Gm.p), h.ldc = naux;
+    h.alpha = -1.0;
+    gemm_f64(h, 1, s);
     cudaMemcpyAsync(dEdPQ, Gm.p, static_cast<size_t>(naux) * naux * sizeof(double), cudaMemcpyDeviceToHost, s);
   }
   ctx->stats.grad_qchunk = qc;

@@ -38,6 +38,7 @@ namespace {
 constexpr uint32_t kTileBytes = 64 * 64 * 2;  // one 64 x 64 bf16 tile
 constexpr int kTcThreads = 192;               // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int kSmemBudget = 225 * 1024;
+constexpr long kMixedMaxOcc = 192;  // orbitals of one half-transform batch (the MMA N of k_xform_tc)
 
 __host__ __device__ inline int tri2(int I, int J) { return I * (I + 1) / 2 + J; }
 
@@ -845,138 +846,146 @@ int mixed_prepare(rijk_ctx* ctx) {
   return RIJK_OK;
 }
 
-int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
-  int rc = mixed_prepare(ctx);
-  if (rc) return rc;
-  const long n = ctx->n, naux = ctx->nq;
-  const long nt2 = round_up(ctx->nt, 2), ntile2 = nt2 * (nt2 + 1) / 2, npad2 = nt2 * TILE;
-  const long noccp = round_up(nocc, 16);
-  const long kdim = naux * noccp;
-  const long nb = nt2 / 2, ntile128 = nb * (nb + 1) / 2;
-  // split-K: chunk-aligned ranges, at least ~4 CTAs per SM in total, every split non-empty; the
-  // split count is chosen in [want, 4 want] so that the CTAs fill whole waves (one CTA per SM)
+// Split-K plan of one SYRK launch: chunk-aligned ranges of `kper` columns, at least ~4 CTAs (or CTA
+// pairs) per SM (pair) in total, every split non-empty; the split count is chosen in [want, 4 want] so
+// that the CTAs fill whole waves.
+struct SyrkPlan {
+  long kper;
+  int nsplit;
+};
+static SyrkPlan syrk_plan(long kdim, long tiles, long slots) {
   const long nchunks = (kdim + 63) / 64;
-  const long sms = num_sms(ctx->device);
-  const long want = std::max<long>(1, (4L * sms + ntile128 - 1) / ntile128);
+  const long want = std::max<long>(1, (4L * slots + tiles - 1) / tiles);
   long best = want;
   double best_eff = 0.0;
   for (long sp = want; sp <= 4 * want && sp <= std::max<long>(1, nchunks / 2); ++sp) {
-    const long ctas = ntile128 * sp, waves = (ctas + sms - 1) / sms;
-    const double eff = static_cast<double>(ctas) / static_cast<double>(waves * sms);
+    const long ctas = tiles * sp, waves = (ctas + slots - 1) / slots;
+    const double eff = static_cast<double>(ctas) / static_cast<double>(waves * slots);
     if (eff > best_eff + 0.02) {  // prefer fewer splits unless the fill improves noticeably
       best_eff = eff;
       best = sp;
     }
   }
-  const long per = std::max<long>(2, (nchunks + best - 1) / best);
-  const long kper = per * 64;
-  const int nsplit = static_cast<int>((kdim + kper - 1) / kper);
+  const long kper = std::max<long>(2, (nchunks + best - 1) / best) * 64;
+  return {kper, static_cast<int>((kdim + kper - 1) / kper)};
+}
+
+// K = sum over orbital batches of X_b^T X_b.  The half-transform holds all orbitals of one batch in
+// the MMA's N dimension (at most 192), so n_c beyond that runs as several batches of equal size; each
+// batch's split-K partials go to their own slots and one reduction sums them all.
+int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
+  int rc = mixed_prepare(ctx);
+  if (rc) return rc;
+  const long n = ctx->n, naux = ctx->nq;
+  const long nt2 = round_up(ctx->nt, 2), ntile2 = nt2 * (nt2 + 1) / 2, npad2 = nt2 * TILE;
+  const long nb = nt2 / 2, ntile128 = nb * (nb + 1) / 2;
+  const long sms = num_sms(ctx->device);
   // K on CTA pairs with 256 x 256 tiles once npad2 >= 1024 (at most one half-empty panel, <= 12.5 %
   // wasted); its split count fills whole waves of SM pairs the same way
   const bool pair_syrk = npad2 >= 1024;
-  const long nb256 = (npad2 + 255) / 256, tiles256 = nb256 * (nb256 + 1) / 2, pairs = sms / 2;
-  long best2 = std::max<long>(1, (4L * pairs + tiles256 - 1) / tiles256);
-  {
-    const long want2 = best2;
-    double eff2 = 0.0;
-    for (long sp = want2; sp <= 4 * want2 && sp <= std::max<long>(1, nchunks / 2); ++sp) {
-      const long n2 = tiles256 * sp, waves = (n2 + pairs - 1) / pairs;
-      const double eff = static_cast<double>(n2) / static_cast<double>(waves * pairs);
-      if (eff > eff2 + 0.02) {
-        eff2 = eff;
-        best2 = sp;
-      }
-    }
+  const long nb256 = (npad2 + 255) / 256, tiles256 = nb256 * (nb256 + 1) / 2;
+  const long nbatch = (round_up(nocc, 16) + kMixedMaxOcc - 1) / kMixedMaxOcc;
+  const long per_batch = round_up((nocc + nbatch - 1) / nbatch, 16);
+  long noccp_max = 0;
+  int nsplit_total = 0;
+  for (long b0 = 0; b0 < nocc; b0 += per_batch) {
+    const long noccp_b = round_up(std::min(per_batch, nocc - b0), 16);
+    noccp_max = std::max(noccp_max, noccp_b);
+    const SyrkPlan pl = pair_syrk ? syrk_plan(naux * noccp_b, tiles256, sms / 2) : syrk_plan(naux * noccp_b, ntile128, sms);
+    nsplit_total += pl.nsplit;
   }
-  const long kper2 = std::max<long>(2, (nchunks + best2 - 1) / best2) * 64;
-  const int nsplit2 = static_cast<int>((kdim + kper2 - 1) / kper2);
-  const int nsplit_k = pair_syrk ? nsplit2 : nsplit;
   cudaStream_t s = ctx->stream;
-  if ((rc = ensure(ctx, ctx->MOp, static_cast<size_t>(2 * noccp * npad2) * sizeof(__nv_bfloat16), "split C")) ||
-      (rc = ensure(ctx, ctx->XT, static_cast<size_t>(2 * npad2) * kdim * sizeof(__nv_bfloat16), "split XT")) ||
-      (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(ntile2) * TILE2 * (sizeof(double) + nsplit_k * sizeof(float)),
-                   "Kpart")))  // fp64 sum area, then the fp32 split partials
-    return rc;
+  if ((rc = ensure(ctx, ctx->MOp, static_cast<size_t>(2 * noccp_max * npad2) * sizeof(__nv_bfloat16), "split C")) ||
+      (rc = ensure(ctx, ctx->XT, static_cast<size_t>(2 * npad2) * naux * noccp_max * sizeof(__nv_bfloat16),
+                   "split XT")) ||
+      (rc = ensure(ctx, ctx->Kpart,
+                   static_cast<size_t>(ntile2) * TILE2 * (sizeof(double) + nsplit_total * sizeof(float)), "Kpart")))
+    return rc;  // fp64 sum area, then the fp32 split partials of every batch
   double* Ksum = static_cast<double*>(ctx->Kpart.p);
   float* Kpart32 = reinterpret_cast<float*>(Ksum + ntile2 * TILE2);
   __nv_bfloat16* Cmix = static_cast<__nv_bfloat16*>(ctx->MOp.p);
   __nv_bfloat16* XT = static_cast<__nv_bfloat16*>(ctx->XT.p);
   int launches = 0;
-  {
-    long total = noccp * npad2;
-    unsigned g = static_cast<unsigned>(std::min<long>((total + 255) / 256, 148L * 16));
-    k_split_c<<<g, 256, 0, s>>>(dMO, nocc, n, noccp, npad2, Cmix);
+  int slot = 0;  // first split slot of the current batch
+  for (long b0 = 0; b0 < nocc; b0 += per_batch) {
+    const long nocc_b = std::min(per_batch, nocc - b0);
+    const long noccp = round_up(nocc_b, 16);
+    const long kdim = naux * noccp;
+    {
+      long total = noccp * npad2;
+      unsigned g = static_cast<unsigned>(std::min<long>((total + 255) / 256, 148L * 16));
+      k_split_c<<<g, 256, 0, s>>>(dMO + b0 * n, nocc_b, n, noccp, npad2, Cmix);
+      ++launches;
+      prof_mark(ctx, "split_c");
+    }
+    CUtensorMap mB, mC, mX;
+    if (!make_map(&mB, ctx->Bmix.p, 64, static_cast<uint64_t>(naux) * ntile2 * 128, 64) ||
+        !make_map(&mC, Cmix, static_cast<uint64_t>(npad2), static_cast<uint64_t>(2 * noccp), static_cast<uint32_t>(noccp)) ||
+        !make_map(&mX, XT, static_cast<uint64_t>(kdim), static_cast<uint64_t>(2 * npad2), 128))
+      return set_err(ctx, RIJK_ERR_CUDA, "tensor map encoding failed");
+    XformParams xp{};
+    xp.nt2 = static_cast<int>(nt2);
+    xp.ntile2 = static_cast<int>(ntile2);
+    xp.naux = static_cast<int>(naux);
+    xp.npairs = static_cast<int>(nb);
+    xp.kdim = kdim;
+    xp.XTh = XT;
+    xp.XTl = XT + npad2 * kdim;
+    xp.err = static_cast<int*>(ctx->err.p);
+    kXformTable[noccp / 16](mB, mC, xp, ctx->device, s);
     ++launches;
-    prof_mark(ctx, "split_c");
-  }
-  CUtensorMap mB, mC, mX;
-  if (!make_map(&mB, ctx->Bmix.p, 64, static_cast<uint64_t>(naux) * ntile2 * 128, 64) ||
-      !make_map(&mC, Cmix, static_cast<uint64_t>(npad2), static_cast<uint64_t>(2 * noccp), static_cast<uint32_t>(noccp)) ||
-      !make_map(&mX, XT, static_cast<uint64_t>(kdim), static_cast<uint64_t>(2 * npad2), 128))
-    return set_err(ctx, RIJK_ERR_CUDA, "tensor map encoding failed");
-  XformParams xp{};
-  xp.nt2 = static_cast<int>(nt2);
-  xp.ntile2 = static_cast<int>(ntile2);
-  xp.naux = static_cast<int>(naux);
-  xp.npairs = static_cast<int>(nb);
-  xp.kdim = kdim;
-  xp.XTh = XT;
-  xp.XTl = XT + npad2 * kdim;
-  xp.err = static_cast<int*>(ctx->err.p);
-  kXformTable[noccp / 16](mB, mC, xp, ctx->device, s);
-  ++launches;
-  prof_mark(ctx, "xform_tc");
-  if (pair_syrk) {
-    SyrkPairParams pp{};
-    pp.kdim = kdim;
-    pp.kper = kper2;
-    pp.npad2 = static_cast<int>(npad2);
-    pp.nt2 = static_cast<int>(nt2);
-    pp.ntile64 = static_cast<int>(ntile2);
-    pp.Kpart = Kpart32;
-    pp.err = static_cast<int*>(ctx->err.p);
-    pp.seg = kSySeg;
-    pp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
-    const size_t smem2 = static_cast<size_t>(pp.stages) * kSyStage + 1024 + 256;
-    ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_tc2), smem2);
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(static_cast<unsigned>(2 * tiles256), static_cast<unsigned>(nsplit2));
-    cfg.blockDim = dim3(kPairThreads);
-    cfg.dynamicSmemBytes = smem2;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = 2;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    rc = cuda_check(ctx, cudaLaunchKernelEx(&cfg, k_syrk_tc2, mX, pp), "CTA-pair SYRK launch");
-    if (rc) return rc;
+    prof_mark(ctx, "xform_tc");
+    float* part = Kpart32 + static_cast<size_t>(slot) * ntile2 * TILE2;
+    if (pair_syrk) {
+      const SyrkPlan pl = syrk_plan(kdim, tiles256, sms / 2);
+      SyrkPairParams pp{};
+      pp.kdim = kdim;
+      pp.kper = pl.kper;
+      pp.npad2 = static_cast<int>(npad2);
+      pp.nt2 = static_cast<int>(nt2);
+      pp.ntile64 = static_cast<int>(ntile2);
+      pp.Kpart = part;
+      pp.err = static_cast<int*>(ctx->err.p);
+      pp.seg = kSySeg;
+      pp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
+      const size_t smem2 = static_cast<size_t>(pp.stages) * kSyStage + 1024 + 256;
+      ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_tc2), smem2);
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(static_cast<unsigned>(2 * tiles256), static_cast<unsigned>(pl.nsplit));
+      cfg.blockDim = dim3(kPairThreads);
+      cfg.dynamicSmemBytes = smem2;
+      cfg.stream = s;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 2;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      rc = cuda_check(ctx, cudaLaunchKernelEx(&cfg, k_syrk_tc2, mX, pp), "CTA-pair SYRK launch");
+      if (rc) return rc;
+      slot += pl.nsplit;
+    } else {
+      const SyrkPlan pl = syrk_plan(kdim, ntile128, sms);
+      SyrkParams sp{};
+      sp.kdim = kdim;
+      sp.kper = pl.kper;
+      sp.npad2 = static_cast<int>(npad2);
+      sp.ntile64 = static_cast<int>(ntile2);
+      sp.Kpart = part;
+      sp.err = static_cast<int*>(ctx->err.p);
+      sp.seg = kSySeg;
+      sp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
+      size_t smem = static_cast<size_t>(sp.stages) * kSyStage + 1024 + 256;
+      ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_tc), smem);
+      dim3 grid(static_cast<unsigned>(ntile128), static_cast<unsigned>(pl.nsplit));
+      k_syrk_tc<<<grid, kTcThreads, smem, s>>>(mX, sp);
+      slot += pl.nsplit;
+    }
     ++launches;
     prof_mark(ctx, "syrk_tc");
-    launch_unpack_sym_f32(Kpart32, nsplit2, ntile2, n, Ksum, dK, s);
-    launches += 2;
-    prof_mark(ctx, "unpack_k");
-    ctx->stats.kernels_last_fock = launches;
-    return cuda_check(ctx, cudaGetLastError(), "mixed exchange launch");
   }
-  SyrkParams sp{};
-  sp.kdim = kdim;
-  sp.kper = kper;
-  sp.npad2 = static_cast<int>(npad2);
-  sp.ntile64 = static_cast<int>(ntile2);
-  sp.Kpart = Kpart32;
-  sp.err = static_cast<int*>(ctx->err.p);
-  sp.seg = kSySeg;
-  sp.stages = std::min(4, static_cast<int>((kSmemBudget - 2048) / kSyStage));
-  size_t smem = static_cast<size_t>(sp.stages) * kSyStage + 1024 + 256;
-  ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_tc), smem);
-  dim3 grid(static_cast<unsigned>(ntile128), static_cast<unsigned>(nsplit));
-  k_syrk_tc<<<grid, kTcThreads, smem, s>>>(mX, sp);
-  ++launches;
-  prof_mark(ctx, "syrk_tc");
-  launch_unpack_sym_f32(Kpart32, nsplit, ntile2, n, Ksum, dK, s);
+  launch_unpack_sym_f32(Kpart32, nsplit_total, ntile2, n, Ksum, dK, s);
   launches += 2;
   prof_mark(ctx, "unpack_k");
   ctx->stats.kernels_last_fock = launches;

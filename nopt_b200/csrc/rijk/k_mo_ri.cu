@@ -7,7 +7,7 @@
 // The reference forms each as C1 (mu nu|P), a product with V^-1/2 over P, a transpose and a
 // second product with C2.  Here B (metric already applied, kept in HBM) is half-transformed by
 // the FP64 DMMA kernel of the Fock build (X^Q = C2 B^Q, all aux functions per launch), the
-// second orbital index comes from one DGEMM over the AO index, and a gather writes the
+// second orbital index comes from one DMMA GEMM over the AO index (k_gemm.cu), and a gather writes the
 // reference's index order.  With RIJK_METRIC_INVSQRT the tensors equal the reference's; with the
 // Cholesky form they differ by an orthogonal rotation of Q, and every contraction over Q agrees.
 #include <algorithm>
@@ -102,11 +102,13 @@ double* half_xform(rijk_ctx* ctx, Scratch& sc, const double* rows2, long p2, int
 // R[r][Q p2 + a] = sum_nu rows1[r0 + r][nu] XT[nu][Q p2 + a], r < nb.
 int second_xform(rijk_ctx* ctx, const double* XT, long p2, const double* rows1, long r0, long nb, double* R) {
   const long npad = ctx->npad, kdim = ctx->nq * p2;
-  const double one = 1.0, zero = 0.0;
-  cublasStatus_t st = cublasDgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_N, static_cast<int>(kdim), static_cast<int>(nb),
-                                  static_cast<int>(npad), &one, XT, static_cast<int>(kdim), rows1 + r0 * npad,
-                                  static_cast<int>(npad), &zero, R, static_cast<int>(kdim));
-  return st == CUBLAS_STATUS_SUCCESS ? RIJK_OK : set_err(ctx, RIJK_ERR_CUDA, "DGEMM of the second transform failed");
+  GemmF64Args g;
+  g.M = nb, g.N = kdim, g.K = npad;
+  g.A = rows1 + r0 * npad, g.lda = npad, g.a_kmajor = true;
+  g.B = XT, g.ldb = kdim, g.b_kmajor = false;
+  g.C = R, g.ldc = kdim;
+  gemm_f64(g, 1, ctx->stream);
+  return cuda_check(ctx, cudaGetLastError(), "second transform");
 }
 
 // out (host) [(p n2 + a)][Q] for all rows p of rows1 (n1 of them), in row blocks of <= ~1 GiB.
@@ -257,11 +259,14 @@ RIJK_API int rijk_mo_ints_aaag(rijk_ctx* ctx, double* MO_INTS, const double* MO_
   const long m = n_a * n_mo, nn = n_a * n_a;
   double* M = sc.get(ctx, static_cast<size_t>(m) * nn, "AAAG integrals", &rc);
   if (rc) return rc;
-  const double one = 1.0, zero = 0.0;
-  if (cublasDgemm(ctx->cublas, CUBLAS_OP_T, CUBLAS_OP_N, static_cast<int>(m), static_cast<int>(nn), static_cast<int>(naux),
-                  &one, Z, static_cast<int>(naux), ap.Yt, static_cast<int>(naux), &zero, M,
-                  static_cast<int>(m)) != CUBLAS_STATUS_SUCCESS)
-    return set_err(ctx, RIJK_ERR_CUDA, "DGEMM of the AAAG contraction failed");
+  {  // M[(t u)][(v x)] = sum_Q Yt[(t u)][Q] Z[(v x)][Q]
+    GemmF64Args g;
+    g.M = nn, g.N = m, g.K = naux;
+    g.A = ap.Yt, g.lda = naux, g.a_kmajor = true;
+    g.B = Z, g.ldb = naux, g.b_kmajor = true;
+    g.C = M, g.ldc = m;
+    gemm_f64(g, 1, ctx->stream);
+  }
   rc = cuda_check(ctx, cudaMemcpyAsync(MO_INTS, M, static_cast<size_t>(m) * nn * sizeof(double), cudaMemcpyDeviceToHost,
                                        ctx->stream), "D2H AAAG integrals");
   if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "rijk_mo_ints_aaag");
@@ -279,16 +284,18 @@ RIJK_API int rijk_soscf_hess_ints(rijk_ctx* ctx, double* aa_J, double* aa_K, con
   Scratch sc;
   ActiveParts ap;
   if ((rc = active_parts(ctx, sc, MO_VEC, n_c, n_a, n_mo, ap))) return rc;
-  const double one = 1.0, zero = 0.0;
   // aa_K[p][t][u] = sum_Q (p t|Q)(p u|Q): one n_a x n_a product per orbital p
   double* dK = sc.get(ctx, static_cast<size_t>(n_mo) * n_a * n_a, "aa_K", &rc);
   if (rc) return rc;
   const long kdim = naux * ap.p2;
-  if (cublasDgemmStridedBatched(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_T, static_cast<int>(n_a), static_cast<int>(n_a),
-                                static_cast<int>(naux), &one, ap.R_all, static_cast<int>(ap.p2), kdim, ap.R_all,
-                                static_cast<int>(ap.p2), kdim, &zero, dK, static_cast<int>(n_a), n_a * n_a,
-                                static_cast<int>(n_mo)) != CUBLAS_STATUS_SUCCESS)
-    return set_err(ctx, RIJK_ERR_CUDA, "batched DGEMM of aa_K failed");
+  {
+    GemmF64Args g;
+    g.M = n_a, g.N = n_a, g.K = naux;
+    g.A = ap.R_all, g.lda = ap.p2, g.sA = kdim, g.a_kmajor = false;
+    g.B = ap.R_all, g.ldb = ap.p2, g.sB = kdim, g.b_kmajor = false;
+    g.C = dK, g.ldc = n_a, g.sC = n_a * n_a;
+    gemm_f64(g, n_mo, ctx->stream);
+  }
   // (pp|Q) for every orbital, by half-transforms of batches of rows
   double* Rpp = sc.get(ctx, static_cast<size_t>(n_mo) * naux, "(pp|Q)", &rc);
   if (rc) return rc;
@@ -309,10 +316,14 @@ RIJK_API int rijk_soscf_hess_ints(rijk_ctx* ctx, double* aa_J, double* aa_K, con
   // aa_J[p][(t u)] = sum_Q (pp|Q)(t u|Q)
   double* dJ = sc.get(ctx, static_cast<size_t>(n_mo) * n_a * n_a, "aa_J", &rc);
   if (rc) return rc;
-  if (cublasDgemm(ctx->cublas, CUBLAS_OP_T, CUBLAS_OP_N, static_cast<int>(n_a * n_a), static_cast<int>(n_mo),
-                  static_cast<int>(naux), &one, ap.Yt, static_cast<int>(naux), Rpp, static_cast<int>(naux), &zero, dJ,
-                  static_cast<int>(n_a * n_a)) != CUBLAS_STATUS_SUCCESS)
-    return set_err(ctx, RIJK_ERR_CUDA, "DGEMM of aa_J failed");
+  {
+    GemmF64Args g;
+    g.M = n_mo, g.N = n_a * n_a, g.K = naux;
+    g.A = Rpp, g.lda = naux, g.a_kmajor = true;
+    g.B = ap.Yt, g.ldb = naux, g.b_kmajor = true;
+    g.C = dJ, g.ldc = n_a * n_a;
+    gemm_f64(g, 1, ctx->stream);
+  }
   const size_t bytes = static_cast<size_t>(n_mo) * n_a * n_a * sizeof(double);
   rc = cuda_check(ctx, cudaMemcpyAsync(aa_J, dJ, bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H aa_J");
   if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(aa_K, dK, bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H aa_K");

@@ -6,8 +6,9 @@
 // takes MO_INTS = RI_aa RI_aa^T over the aux index.  With B already fitted:
 //     Y^Q = C1 B^Q C2^T  (n_a x n_a),   MO_INTS[(b n_a + a) n_a^2 + d n_a + c] = sum_Q Y^Q_ab Y^Q_cd
 // (a, c from MO_VEC1; b, d from MO_VEC2, as the reference's RI_aa index order (b, a)).
-// Device work: the FP64 half-transform kernel (C1 as the orbital block), a strided-batched
-// DGEMM per aux function for Y^Q, one DGEMM Z Z^T over Q, and a gather into the reference's order.
+// Device work: the FP64 half-transform kernel (C1 as the orbital block), a batched DMMA GEMM
+// (k_gemm.cu) with one product per aux function for Y^Q, one GEMM Z Z^T over Q, and a gather into
+// the reference's order.
 // The core J and K come from the ordinary FP64 Fock build with D_core and the first n_c rows of
 // MO_VEC, exactly the reference's tail (src/RI.cpp:235-287).
 #include <vector>
@@ -70,7 +71,6 @@ RIJK_API int rijk_mo_ints(rijk_ctx* ctx, const double* DM_D, double* J, double* 
   }
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
-  cublasHandle_t cb = ctx->cublas;
   const long n = ctx->n, naux = ctx->nq, npad = ctx->npad, nt = ctx->nt;
   const long p = round_up(n_a, 16), kdim = naux * p, p2 = p * p;
   const size_t cbytes = static_cast<size_t>(n_a) * n * sizeof(double);
@@ -101,16 +101,22 @@ RIJK_API int rijk_mo_ints(rijk_ctx* ctx, const double* DM_D, double* J, double* 
   // X1^Q: XT[nu][Q p + a] = sum_mu B^Q_{nu mu} C1_{a mu}
   launch_xform_f64(static_cast<const double*>(ctx->B.p), static_cast<const double*>(R1.p), naux, nt, p,
                    static_cast<double*>(XTa.p), s);
-  const double one = 1.0, zero = 0.0;
-  const int pi = static_cast<int>(p), npi = static_cast<int>(npad);
-  // Y^Q (p x p, column-major: Y[a + b p]) = X1^Q (p x npad, ld kdim) . R2 (as npad x p column-major)
-  cublasDgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_N, pi, pi, npi, &one, static_cast<const double*>(XTa.p),
-                            static_cast<int>(kdim), p, static_cast<const double*>(R2.p), npi, 0, &zero,
-                            static_cast<double*>(Y.p), pi, p2, static_cast<int>(naux));
-  // G = Z Z^T with Z (p^2 x naux) column-major = the Y buffer
-  const int p2i = static_cast<int>(p2);
-  cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, p2i, p2i, static_cast<int>(naux), &one, static_cast<const double*>(Y.p),
-              p2i, static_cast<const double*>(Y.p), p2i, &zero, static_cast<double*>(G.p), p2i);
+  {  // Y^Q[b][a] = sum_nu C2_{b nu} X1^Q_{a nu}  (p x p per aux function)
+    GemmF64Args g;
+    g.M = p, g.N = p, g.K = npad;
+    g.A = static_cast<const double*>(R2.p), g.lda = npad, g.sA = 0, g.a_kmajor = true;
+    g.B = static_cast<const double*>(XTa.p), g.ldb = kdim, g.sB = p, g.b_kmajor = false;
+    g.C = static_cast<double*>(Y.p), g.ldc = p, g.sC = p2;
+    gemm_f64(g, naux, s);
+  }
+  {  // G[x][y] = sum_Q Y^Q[x] Y^Q[y] over the flattened p^2 entries
+    GemmF64Args g;
+    g.M = p2, g.N = p2, g.K = naux;
+    g.A = static_cast<const double*>(Y.p), g.lda = p2, g.a_kmajor = false;
+    g.B = static_cast<const double*>(Y.p), g.ldb = p2, g.b_kmajor = false;
+    g.C = static_cast<double*>(G.p), g.ldc = p2;
+    gemm_f64(g, 1, s);
+  }
   k_gather_moints<<<grid_of(n_a * n_a * n_a * n_a), 256, 0, s>>>(static_cast<const double*>(G.p), n_a, p,
                                                                    static_cast<double*>(out.p));
   cudaMemcpyAsync(MO_INTS, out.p, static_cast<size_t>(n_a * n_a) * n_a * n_a * sizeof(double), cudaMemcpyDeviceToHost,

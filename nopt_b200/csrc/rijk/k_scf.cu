@@ -454,6 +454,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: guess needs factor rows (1 .. n_ao of them)");
   if (ctx->nq != ctx->naux)
     return set_err(ctx, RIJK_ERR_STATE, "rijk_scf needs all aux functions in one context (no aux range)");
+  if (o.ao_projector && (o.n_proj < 1 || o.n_proj > ctx->n))
+    return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: n_proj = %ld outside [1, n_ao = %ld]", o.n_proj, ctx->n);
   cudaSetDevice(ctx->device);
   const auto t_start = std::chrono::steady_clock::now();
   const long n = ctx->n, nn = n * n;
@@ -462,7 +464,6 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   cublasHandle_t cb = ctx->cublas;
   cusolverDnHandle_t cs = ctx->cusolver;
   const int m_max = o.diis_size;
-  constexpr long kMixedRows = 192;  // orbitals one mixed build takes
 
   // Work buffers live in the context between calls (grown as needed, freed by rijk_destroy): an SCF
   // call then makes no cudaMalloc / cudaFree, whose frees synchronise the device.
@@ -543,14 +544,32 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   }
   double* pWork = static_cast<double*>(work.p);
 
-  // X = U_k w_k^-1/2 over eigenvalues of S above lindep (ascending: drop the first ndrop)
-  cudaMemcpyAsync(pU, pS, b_nn, cudaMemcpyDeviceToDevice, s);
-  if (cusolverDnDsyevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, ni, pU, ni, pW, pWork, lwork, pInfo) !=
+  // X = U_k w_k^-1/2 over eigenvalues of S above lindep (ascending: drop the first ndrop).  With a
+  // projector T (n x np), the same from S' = T^T S T, and X = T U'_k w'_k^-1/2: the orbitals then
+  // lie in the span of T's columns (the reference's D5 treatment).
+  const bool proj = o.ao_projector != nullptr;
+  const long np = proj ? o.n_proj : n;
+  const int npi = static_cast<int>(np);
+  DeviceBuf& dP = wb[27];
+  if (proj) {
+    // T row-major (n x np) is, read column-major with ld np, T^T (np x n)
+    if ((rc = ensure(ctx, dP, static_cast<size_t>(n) * np * sizeof(double), "scf projector"))) {
+      cleanup();
+      return rc;
+    }
+    cudaMemcpyAsync(dP.p, o.ao_projector, static_cast<size_t>(n) * np * sizeof(double), cudaMemcpyHostToDevice, s);
+    const double* pP = static_cast<const double*>(dP.p);
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_T, ni, npi, ni, &one, pS, ni, pP, npi, &zero, pT1, ni);   // S T
+    cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, npi, npi, ni, &one, pP, npi, pT1, ni, &zero, pU, npi);  // T^T S T
+  } else {
+    cudaMemcpyAsync(pU, pS, b_nn, cudaMemcpyDeviceToDevice, s);
+  }
+  if (cusolverDnDsyevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, npi, pU, npi, pW, pWork, lwork, pInfo) !=
       CUSOLVER_STATUS_SUCCESS)
     return fail(RIJK_ERR_SOLVER, "syevd of S failed");
-  std::vector<double> ws(n);
+  std::vector<double> ws(np);
   int hinfo = 0;
-  cudaMemcpyAsync(ws.data(), pW, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(ws.data(), pW, np * sizeof(double), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(&hinfo, pInfo, sizeof(int), cudaMemcpyDeviceToHost, s);
   if ((rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf overlap"))) {
     cleanup();
@@ -558,11 +577,17 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   }
   if (hinfo != 0) return fail(RIJK_ERR_SOLVER, "overlap eigendecomposition did not converge");
   long first = 0;
-  while (first < n && ws[first] < o.lindep) ++first;
-  const long nm = n - first;
+  while (first < np && ws[first] < o.lindep) ++first;
+  const long nm = np - first;
   if (nm < nocc) return fail(RIJK_ERR_ARG, "fewer independent orbitals than n_c");
   const int nmi = static_cast<int>(nm);
-  k_scale_cols<<<grid_of(n * nm), 256, 0, s>>>(pU, pW, n, first, nm, pX);
+  if (proj) {
+    k_scale_cols<<<grid_of(np * nm), 256, 0, s>>>(pU, pW, np, first, nm, pT2);  // X' (np x nm)
+    cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, ni, nmi, npi, &one, static_cast<const double*>(dP.p), npi, pT2, npi,
+                &zero, pX, ni);  // X = T X'
+  } else {
+    k_scale_cols<<<grid_of(n * nm), 256, 0, s>>>(pU, pW, n, first, nm, pX);
+  }
 
   // Inside the loop only the n_c occupied orbitals are needed: syevdx for the lowest n_c
   // eigenpairs (all of them, with syevd, for the final orbitals).
@@ -687,18 +712,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     cudaMemcpyAsync(dR.p, o.guess_rows, static_cast<size_t>(o.guess_nrows) * n * sizeof(double),
                     cudaMemcpyHostToDevice, s);
     // The guess Fock matrix only seeds the first diagonalisation: a mixed run builds it in the
-    // mixed form, K summed over batches of at most 192 factor rows (K is linear in D = R^T R).
-    if (o.precision == RIJK_PREC_MIXED) {
-      const long nr = o.guess_nrows;
-      const double* R = static_cast<const double*>(dR.p);
-      for (long r0 = 0; r0 < nr && !rc; r0 += kMixedRows) {
-        const long cnt = std::min(kMixedRows, nr - r0);
-        rc = fock_device_impl(ctx, pD, R + r0 * n, cnt, r0 == 0 ? pJ : pT1, r0 == 0 ? pK : pT2, RIJK_PREC_MIXED);
-        if (!rc && r0 > 0) k_axpy_set<<<grid_of(nn), 256, 0, s>>>(1.0, pT2, nn, pK, 0);
-      }
-    } else {
-      rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, o.precision);
-    }
+    // mixed form (the factor rows in orbital batches inside the build).
+    rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, o.precision);
     if (!rc) {
       k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
       rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf guess");

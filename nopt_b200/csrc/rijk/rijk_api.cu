@@ -604,10 +604,6 @@ int check_fock_args(rijk_ctx* ctx, long nocc, int precision) {
     return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld outside [0, n_ao = %ld]", nocc, ctx->n);
   if (precision != RIJK_PREC_FP64 && precision != RIJK_PREC_MIXED && precision != RIJK_PREC_FP64_TC)
     return set_err(ctx, RIJK_ERR_ARG, "unknown precision %d", precision);
-  // the FP64 half-transform runs in orbital batches (any n_c); the tcgen05 form holds all n_c
-  // columns of one aux function in TMEM (N <= 192)
-  if (precision == RIJK_PREC_MIXED && round_up(nocc, 16) > 192)
-    return set_err(ctx, RIJK_ERR_ARG, "n_c = %ld exceeds the 192 of the mixed form", nocc);
   return RIJK_OK;
 }
 }  // namespace rijk

@@ -128,6 +128,28 @@ int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& f
 // with it the array itself, so rijk_create does it while allocating is still allowed.
 int noalloc_resolve(rijk_ctx* ctx);
 
+// ---- k_gemm.cu
+// C_b = alpha op(A_b) op(B_b) + beta C_b for b < batch (FP64 DMMA, 64 x 64 tiles); see k_gemm.cu for
+// the layouts and the GEMM_PAIRS epilogue.  K may be 0 (C = beta C).
+constexpr int GEMM_STORE = 0;
+constexpr int GEMM_PAIRS = 1;
+struct GemmF64Args {
+  long M = 0, N = 0, K = 0;
+  const double* A = nullptr;
+  long lda = 0, sA = 0;
+  bool a_kmajor = true;  // A(m, k) = A[m lda + k]; false: A[k lda + m]
+  const double* B = nullptr;
+  long ldb = 0, sB = 0;
+  bool b_kmajor = true;  // B(k, n) = B[n ldb + k]; false: B[k ldb + n]
+  double* C = nullptr;
+  long ldc = 0, sC = 0;
+  double alpha = 1.0, beta = 0.0;
+  int mode = GEMM_STORE;
+  long n_ao = 0;       // GEMM_PAIRS: orbital functions
+  int kdiag = 0;       // 1: k runs over packed-triangle elements, diagonal tiles weighted 1/2
+};
+void gemm_f64(const GemmF64Args& p, long batch, cudaStream_t s);
+
 // ---- k_pack.cu
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s);

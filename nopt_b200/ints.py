@@ -44,6 +44,7 @@ def lib():
         L.gto_coulomb_3c.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _dp]
         L.gto_boys.argtypes = [ctypes.c_int, ctypes.c_double, _dp]
         L.gto_atomic_density.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, _dp, _dp, _dp, _ip]
+        L.gto_cart_to_sph.argtypes = [ctypes.c_int, _dp]
         L.gto_set_threads.argtypes = [ctypes.c_int]
         L.gto_set_threads.restype = None
         _LIB = L
@@ -134,6 +135,31 @@ def coulomb_3c(orb, aux, layout=LAYOUT_PACKED):
         out = np.empty((n * (n + 1) // 2, na))
     _check(lib().gto_coulomb_3c(orb._h, aux._h, layout, _ptr(out)), "gto_coulomb_3c")
     return out
+
+
+def cart_to_sph(l):
+    """(2l+1) x ncart(l) matrix C, Y_m = sum_c C[m][c] phi_c (gto_cart_to_sph)."""
+    nc = (l + 1) * (l + 2) // 2
+    out = np.empty((2 * l + 1, nc))
+    _check(lib().gto_cart_to_sph(int(l), _ptr(out)), "gto_cart_to_sph")
+    return out
+
+
+def d5_projector(cart):
+    """T (n_cart x n_sph) for a Cartesian basis: column j is spherical function j of the same shells in
+    terms of the Cartesian functions, shell by shell (the role of the reference's T_D5,
+    src/molecule.cpp:4551-4680).  T^T S_cart T is the overlap of the spherical basis."""
+    if cart.pure:
+        raise ValueError("d5_projector needs a Cartesian basis")
+    nsph = sum(2 * sh.l + 1 for sh in cart.shells)
+    T = np.zeros((cart.nbf, nsph))
+    r = c = 0
+    for sh in cart.shells:
+        C = cart_to_sph(sh.l)
+        T[r:r + C.shape[1], c:c + C.shape[0]] = C.T
+        r += C.shape[1]
+        c += C.shape[0]
+    return T
 
 
 def aux_slice_bounds(aux, nslices):

@@ -65,7 +65,7 @@ class ScfOpts(ctypes.Structure):
                 ("guess_dm", _dp), ("guess_rows", _dp), ("guess_nrows", ctypes.c_long),
                 ("converger", ctypes.c_int), ("conv_grad", ctypes.c_double), ("conv_energy", ctypes.c_double),
                 ("lbfgs_vectors", ctypes.c_int), ("density_by_eigenvectors", ctypes.c_int),
-                ("fp64_phase_precision", ctypes.c_int)]
+                ("fp64_phase_precision", ctypes.c_int), ("ao_projector", _dp), ("n_proj", ctypes.c_long)]
 
 
 class ScfResult(ctypes.Structure):
@@ -281,14 +281,16 @@ class FockBuilder:
 
     def scf(self, H, S, n_c, e_nuc, precision=PREC_FP64, conv_dm_rms=1e-10, switch_diis_err=1e-5, max_iter=100,
             diis_size=8, guess=None, diis_keep_on_switch=False, converger=CONV_DIIS, conv_grad=1e-7,
-            conv_energy=1e-10, lbfgs_vectors=0, purify=True, fp64_phase=PREC_FP64):
+            conv_energy=1e-10, lbfgs_vectors=0, purify=True, fp64_phase=PREC_FP64, projector=None):
         """RHF on the GPU (rijk_scf); guess = (D0, R) with D0 = R^T R (e.g. SystemIntegrals.sad()),
         None for the core-Hamiltonian start; converger CONV_DIIS, CONV_SOSCF (the reference's
         L-BFGS orbital rotations, converged on max|4 F_ai| < conv_grad or |dE| < conv_energy), or
         CONV_DIIS_SOSCF (DIIS while the builds are mixed, SOSCF from the switch to FP64 on).
         purify=False diagonalises X^T F X at every DIIS step (the reference's step); the default
         takes the occupied space from purification, with the eigensolver as its fallback.
-        fp64_phase=PREC_FP64_TC makes the builds after a mixed phase FP64_TC ones.
+        fp64_phase=PREC_FP64_TC makes the builds after a mixed phase FP64_TC ones.  projector (n x n_proj)
+        confines the orbitals to the span of its columns, e.g. the Cartesian->spherical map of a
+        Cartesian orbital basis (ints.d5_projector), as the reference's D5 treatment.
         Returns (E, MO rows, result dict)."""
         n = self.n
         o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1 if diis_keep_on_switch else 0,
@@ -299,6 +301,9 @@ class FockBuilder:
         if guess is not None:
             gD, gR = _c(guess[0]), _c(guess[1])
             o.guess_dm, o.guess_rows, o.guess_nrows = _p(gD), _p(gR), gR.shape[0]
+        if projector is not None:
+            T = _c(projector)
+            o.ao_projector, o.n_proj = _p(T), T.shape[1]
         r = ScfResult()
         MO = np.zeros((n, n))
         rc = lib().rijk_scf(self._h, _p(_c(H)), _p(_c(S)), int(n_c), float(e_nuc), ctypes.byref(o), _p(MO),

@@ -293,15 +293,20 @@ def adjoint_reference(I3_packed, M, H, MO, n_c, Enuc):
 
 
 # --------------------------------------------------------------------- SCF ------
-def scf_rhf(S, H, RI_AA, Vm05, n_occ, Enuc, conv_dm=1e-10, max_iter=100, diis_n=8, jk=None, guess=None):
+def scf_rhf(S, H, RI_AA, Vm05, n_occ, Enuc, conv_dm=1e-10, max_iter=100, diis_n=8, jk=None, guess=None,
+            projector=None):
     """Restricted HF with DIIS on F D S - S D F, using the reference's J/K, F and E
     conventions.  Returns (E, MO, DM, F, iterations).  `jk(DM, MO, n_rows) -> (J, K)` overrides
     the Fock build (default: dm_to_f_transform_ri on RI_AA/Vm05); `guess = (D0, R)` starts from
-    the Fock matrix of D0 = R^T R instead of the core Hamiltonian."""
+    the Fock matrix of D0 = R^T R instead of the core Hamiltonian.  `projector` T (n x n_proj)
+    confines the orbitals to its columns' span: every diagonalisation is the generalised problem
+    (T^T F T) V = (T^T S T) V e with MO = V^T T^T, as diag_X_AO_in_MO with D5 = 1
+    (src/molecule.cpp:4004-4050)."""
     n = S.shape[0]
-    s, U = np.linalg.eigh(S)
+    T = np.eye(n) if projector is None else projector
+    s, U = np.linalg.eigh(T.T @ S @ T)
     keep = s > 1e-10
-    X = U[:, keep] / np.sqrt(s[keep])
+    X = T @ (U[:, keep] / np.sqrt(s[keep]))
     if jk is None:
         jk = lambda D, MO, nr=n_occ: dm_to_f_transform_ri(RI_AA, Vm05, D, MO, nr, n)
 

@@ -9,7 +9,7 @@ and writes them with their source file:line.  It also reads the normalised contr
 coefficients the reference prints for the carbon shells of C2H4 (column "c" of the basis
 table), which pin the basis normalisation.
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference tree>
 """
 import json
 import os
@@ -97,4 +97,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <path of the reference tree>")
+    main(sys.argv[1])

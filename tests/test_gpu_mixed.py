@@ -63,9 +63,11 @@ def test_mixed_k_water_hexamer():
 
 
 @pytest.mark.parametrize("n,naux,nocc", [(200, 96, 97), (64, 40, 16), (150, 70, 1), (200, 96, 161), (260, 48, 192),
-                                         (1000, 40, 48), (1100, 36, 100)])
+                                         (1000, 40, 48), (1100, 36, 100), (300, 64, 282), (260, 48, 193),
+                                         (1000, 40, 390)])
 def test_mixed_k_ragged_random(n, naux, nocc):
-    """n >= 1000 takes the CTA-pair SYRK (256 x 256 tiles); n = 1100 ends in a half-filled panel."""
+    """n >= 1000 takes the CTA-pair SYRK (256 x 256 tiles); n = 1100 ends in a half-filled panel.
+    n_c above 192 runs in orbital batches (282 -> 2 x 144, 193 -> 2 x 112, 390 -> 3 x 144)."""
     rng = np.random.default_rng(n)
     A = rng.normal(size=(naux, naux))
     V = A @ A.T / naux + np.eye(naux)

@@ -188,3 +188,33 @@ def test_gpu_scf_fp64_phase_on_int8_tensor_cores():
         assert e.value.code == rijk.ERR_ARG
     assert r64["converged"] and rt["converged"] and rt["iterations_mixed"] > 0
     assert abs(Et - E64) < 1e-9, (Et, E64)
+
+
+@pytest.mark.parametrize("converger", [rijk.CONV_DIIS, rijk.CONV_SOSCF])
+def test_gpu_scf_cartesian_basis_with_d5_projection(converger):
+    """The reference's setting: a Cartesian orbital basis (src/inp_par_read.cpp:2550-2552) with the
+    orbitals confined to the spherical span (D5 = 1, src/molecule.cpp:4004-4050).  The Fock builds
+    run on Cartesian integrals formed on the GPU; rijk_scf with the Cartesian->spherical projector
+    reaches the logged C2H4 energy with both convergers, the orbitals lie in the projector's span,
+    and without the projector the energy is that of the larger Cartesian space."""
+    p = [q for q in GOLD["pins"] if q["name"] == "c2h4"][0]
+    mol = Molecule(p["symbols"], p["coords_ang"])
+    orb = ints.Basis.for_molecule(p["basis"], mol, pure=False)
+    aux = ints.Basis.for_molecule(p["aux"], mol)
+    S, H = ints.overlap(orb), ints.kinetic(orb) + ints.nuclear(orb, mol)
+    T = ints.d5_projector(orb)
+    nocc, Enuc = mol.nelec // 2, mol.nuclear_repulsion()
+    with rijk.FockBuilder(0) as fb:
+        fb.set_basis(orb, aux)
+        E, MO, r = fb.scf(H, S, nocc, Enuc, converger=converger, projector=T)
+        E6, _, r6 = fb.scf(H, S, nocc, Enuc, converger=converger)
+    assert r["converged"] == 1 and r6["converged"] == 1
+    assert r["nmo"] == T.shape[1] and r6["nmo"] == orb.nbf
+    assert abs(E - p["energy"]) < 2e-9, (E, p["energy"])
+    assert E6 < p["energy"] - 1e-4
+    C = MO[:r["nmo"]]
+    assert np.max(np.abs(C @ S @ C.T - np.eye(r["nmo"]))) < 1e-9
+    # in the span of T: C = Z T^T for Z = C S T (T^T S T)^-1
+    Z = C @ S @ T @ np.linalg.inv(T.T @ S @ T)
+    assert np.max(np.abs(Z @ T.T - C)) < 1e-9
+    assert not np.any(MO[r["nmo"]:])

@@ -144,3 +144,22 @@ def test_gram_schmidt_rows_is_qr_with_positive_diagonal():
     Q, Rr = np.linalg.qr(R.T)
     Q = Q * np.sign(np.diag(Rr))
     np.testing.assert_allclose(O.gram_schmidt_rows(R), Q.T, atol=1e-13)
+
+
+def test_cartesian_basis_with_d5_projection_reaches_the_logged_energy():
+    """The reference's orbital basis is Cartesian with D5 = 1 (src/inp_par_read.cpp:2550-2552,
+    src/molecule.cpp:4004-4050): the SCF in the Cartesian AO basis with the orbitals confined to
+    the spherical span reaches the logged C2H4 energy; without the projection it does not."""
+    p = [q for q in GOLD["pins"] if q["name"] == "c2h4"][0]
+    mol = _mol(p)
+    orb = ints.Basis.for_molecule(p["basis"], mol, pure=False)
+    aux = ints.Basis.for_molecule(p["aux"], mol)
+    S, H = ints.overlap(orb), ints.kinetic(orb) + ints.nuclear(orb, mol)
+    RI = ints.coulomb_3c(orb, aux, ints.LAYOUT_NOPT_FULL)
+    Vm05, _ = O.s05_calc(ints.coulomb_2c(aux))
+    nocc = mol.nelec // 2
+    T = ints.d5_projector(orb)
+    E, MO, DM, F, it = O.scf_rhf(S, H, RI, Vm05, nocc, mol.nuclear_repulsion(), projector=T)
+    assert abs(E - p["energy"]) < 2e-9, (E, p["energy"])
+    E6, *_ = O.scf_rhf(S, H, RI, Vm05, nocc, mol.nuclear_repulsion())
+    assert E6 < p["energy"] - 1e-4  # the full Cartesian space holds the extra s-type combinations

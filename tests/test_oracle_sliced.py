@@ -52,3 +52,19 @@ def test_sliced_jk_sums_to_the_full_build():
         K += Ks
     assert np.max(np.abs(J - Jr)) < 1e-11 * max(1.0, np.max(np.abs(Jr)))
     assert np.max(np.abs(K - Kr)) < 1e-11 * max(1.0, np.max(np.abs(Kr)))
+
+
+def test_d5_projector_maps_cartesian_overlap_to_spherical():
+    """T^T S_cart T = S_sph, T^T H_cart T = H_sph: the projected Cartesian space is the spherical one."""
+    from nopt_b200.molecules import Molecule
+    mol = Molecule(["O", "H", "H"], [[0, 0, 0.1173], [0, 0.7572, -0.4692], [0, -0.7572, -0.4692]])
+    for name in ("cc-pvdz", "cc-pvtz"):
+        cart = ints.Basis.for_molecule(name, mol, pure=False)
+        sph = ints.Basis.for_molecule(name, mol, pure=True)
+        T = ints.d5_projector(cart)
+        assert T.shape == (cart.nbf, sph.nbf)
+        Sc, Ss = ints.overlap(cart), ints.overlap(sph)
+        np.testing.assert_allclose(T.T @ Sc @ T, Ss, atol=1e-13)
+        Hc = ints.kinetic(cart) + ints.nuclear(cart, mol)
+        Hs = ints.kinetic(sph) + ints.nuclear(sph, mol)
+        np.testing.assert_allclose(T.T @ Hc @ T, Hs, atol=1e-12)
