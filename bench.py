@@ -330,7 +330,62 @@ def cpu_baseline_for(si, DM, MO, workload, seed, nslices, budget_s):
 
 
 # ------------------------------------------------------------------ GPU arm ------
-def extra_workload(name, seed, dev, steps, want_cpu, budget_s):
+def grad_report(fb, si, MOc, nocc, fp64_peak, reps=3):
+    """rijk_grad (E, dE/dC, dE/d(P|mu nu) packed, dE/d(P|Q); host outputs): wall time per call, and
+    the device time, FLOPs and FP64 roofline fraction of each stage (profiling events)."""
+    from nopt_b200 import rijk
+    fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)  # first call: module loads
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
+    wall = (time.perf_counter() - t0) / reps
+    fb.set_profiling(True)
+    fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
+    fb.set_profiling(False)
+    st = fb.stats()
+    n, naux = si.n, si.naux
+    npad = st["npad"]
+    noccp = (nocc + 15) // 16 * 16
+    te = st["ntile"] * 4096
+    chunked = st["grad_qchunk"] < naux
+    flops = {"x_recompute": 2.0 * noccp * npad * npad * naux if chunked else 0.0,
+             "y_t": 4.0 * noccp * noccp * npad * naux, "gamma": 2.0 * te * noccp * naux,
+             "d3c_M_gamma": 2.0 * te * naux * naux, "g_gamma_B": 2.0 * te * naux * naux, "dV_MtGM": 4.0 * naux ** 3}
+    stages = {}
+    for k, ms in st["grad_stages"].items():
+        e = {"ms": ms}
+        if k in flops and ms > 0 and flops[k] > 0:
+            e["tflops"] = flops[k] / (ms * 1e-3) / 1e12
+            e["frac_of_fp64_peak"] = e["tflops"] / fp64_peak
+        stages[k] = e
+    top = max((k for k in stages if k in flops), key=lambda k: stages[k]["ms"])
+    return {"wall_ms": 1e3 * wall, "device_ms": st["ms_grad_total"], "aux_chunk": st["grad_qchunk"],
+            "recompute_path": bool(chunked), "stages": stages, "top_stage": top,
+            "flops": sum(flops.values()), "fp64_peak_tflops": fp64_peak,
+            "what": "rijk_grad through the C ABI: E, dE/dC, dE/d(P|mu nu) (packed) and dE/d(P|Q) to host memory; "
+                    "device_ms = its kernels before the host copies (stage events), wall_ms includes the copies "
+                    "(%.2f GB) and the call's buffer allocation" % ((n * (n + 1) // 2 * naux + naux * naux) * 8 / 1e9)}
+
+
+def c40h82_grad(seed, dev, fp64_peak, chunk=1200):
+    """BASELINE's C40H82 adjoint case: mixed -> FP64 SCF, then rijk_grad with Gamma in aux chunks and
+    X^Q recomputed in tiles (the path taken when HBM cannot hold Gamma for every aux function)."""
+    from nopt_b200 import rijk
+    si, _, _ = build_system("c40h82_dz", seed, ri_integrals=False)
+    with rijk.FockBuilder(dev.index) as fb:
+        fb.set_basis(si.orb, si.aux, rijk.METRIC_INVSQRT)
+        t0 = time.perf_counter()
+        E, MOc, r = fb.scf(si.H, si.S, si.nocc, si.Enuc, precision=rijk.PREC_MIXED, guess=si.sad(),
+                           converger=rijk.CONV_DIIS_SOSCF)
+        t_scf = time.perf_counter() - t0
+        fb.set_grad_chunk(chunk)
+        g = grad_report(fb, si, MOc, si.nocc, fp64_peak, reps=1)
+    g.update({"workload": WORKLOAD_NAMES["c40h82_dz"], "scf_seconds_first_call": t_scf, "energy": E,
+              "scf_builds": r["iterations"], "scf_builds_mixed": r["iterations_mixed"]})
+    return g
+
+
+def extra_workload(name, seed, dev, steps, want_cpu, budget_s, fp64_peak):
     """A second workload on a fresh context: FP64 and mixed builds/s (device-timed), e2e through
     rijk_fock, SCF times, the adjoint's time, and the CPU arm's builds/s."""
     import ctypes
@@ -398,13 +453,8 @@ def extra_workload(name, seed, dev, steps, want_cpu, budget_s):
         out["scf"] = scf
         # the adjoint (rijk_grad) at the converged FP64 orbitals: E, dE/dC, dE/d(P|mu nu), dE/d(P|Q)
         E, MOc, _ = fb.scf(si.H, si.S, nocc, si.Enuc, guess=guess)
-        fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
-        t0 = time.perf_counter()
-        for _ in range(3):
-            fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
-        out["grad"] = {"ms": 1e3 * (time.perf_counter() - t0) / 3,
-                       "what": "rijk_grad wall time through the C ABI: E, dE/dC, dE/d(P|mu nu) (packed) and dE/d(P|Q), "
-                               "host outputs"}
+        out["grad"] = grad_report(fb, si, MOc, nocc, fp64_peak)
+
     if want_cpu:
         out["cpu_baseline"] = cpu_baseline_for(si, DM, MO, name, seed, 12, budget_s)
         if "value" in out["cpu_baseline"]:
@@ -803,11 +853,14 @@ def main():
     if want_cpu:
         cpu = cpu_baseline_for(si, DM, MO, args.workload, args.seed, args.cpu_slices, args.cpu_seconds)
 
-    extra = scf_small = None
+    extra = scf_small = grad_c40 = None
     if rank == 0 and world == 1 and not synthetic and args.extra not in ("none", "", args.workload):
-        extra = extra_workload(args.extra, args.seed, dev, max(5, args.steps // 2), want_cpu, args.cpu_seconds / 2)
+        extra = extra_workload(args.extra, args.seed, dev, max(5, args.steps // 2), want_cpu, args.cpu_seconds / 2,
+                               fp64_peak)
         if want_cpu and not args.no_scf:
             scf_small = scf_cpu_small(args.seed, dev)
+        if not args.no_scf:
+            grad_c40 = c40h82_grad(args.seed, dev, fp64_peak)
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
@@ -834,6 +887,8 @@ def main():
             out["extra_" + args.extra] = extra
         if scf_small is not None:
             out["scf_cpu_vs_gpu_h2o6"] = scf_small
+        if grad_c40 is not None:
+            out["grad_c40h82"] = grad_c40
         print(json.dumps(out), flush=True)
     if dist is not None:
         dist.destroy_process_group()

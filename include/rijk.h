@@ -83,6 +83,11 @@ typedef struct {
   int kernels_setup_ints; /* integral kernels it launched                                    */
   long q0, nq;            /* aux functions [q0, q0 + nq) held (all of them unless sliced)      */
   long grad_qchunk;       /* aux functions per chunk of the last rijk_grad (naux: one chunk)    */
+  /* Device time of the stages of the last rijk_grad, summed over its aux chunks (with profiling
+   * on): [0] the FP64 Fock build, energy and dE/dC, [1] X^Q recomputed in tiles (0 unless chunked),
+   * [2] Y^Q and T^Q, [3] Gamma, [4] dE/d(P|mu nu) = M^T Gamma, [5] G = Gamma B, [6] -M^T G M.      */
+  double ms_grad_stage[7];
+  double ms_grad_total;   /* device time of rijk_grad before its host copies (profiling on)     */
 } rijk_stats_t;
 
 int rijk_create(rijk_ctx** ctx, int device);

@@ -138,6 +138,36 @@ __global__ void k_energy_partial(const double* __restrict__ D, const double* __r
   }
 }
 
+// Device time per stage of rijk_grad when profiling is on: mark(k) records an event on the stream,
+// and the interval since the previous mark counts for stage k (k < 0: not counted).
+struct GradTimer {
+  bool on = false;
+  cudaStream_t s = nullptr;
+  std::vector<std::pair<int, cudaEvent_t>> ev;
+  void mark(int stage) {
+    if (!on) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    ev.emplace_back(stage, e);
+  }
+  // after the stream has drained
+  void collect(rijk_stats_t& st) {
+    for (double& v : st.ms_grad_stage) v = 0.0;
+    st.ms_grad_total = 0.0;
+    for (size_t i = 1; i < ev.size(); ++i) {
+      if (ev[i].first < 0) continue;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev[i - 1].second, ev[i].second);
+      st.ms_grad_stage[ev[i].first] += ms;
+      st.ms_grad_total += ms;
+    }
+  }
+  ~GradTimer() {
+    for (auto& e : ev) cudaEventDestroy(e.second);
+  }
+};
+
 unsigned grid_of(long total) {
   long b = (total + 255) / 256;
   if (b > 148L * 16) b = 148L * 16;
@@ -190,6 +220,10 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   double* pF = static_cast<double*>(dF.p);
   cudaMemcpyAsync(pMO, MO, nocc * n * sizeof(double), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(dH.p, H, b_nn, cudaMemcpyHostToDevice, s);
+  GradTimer tm;
+  tm.on = ctx->profiling;
+  tm.s = s;
+  tm.mark(-1);
   {  // D[mu][nu] = sum_i C[i][mu] C[i][nu]
     GemmF64Args g;
     g.M = n, g.N = n, g.K = nocc;
@@ -213,9 +247,11 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
     g.alpha = 4.0;
     gemm_f64(g, 1, s);
   }
+  tm.mark(0);
   std::vector<double> part(1024);
   cudaMemcpyAsync(part.data(), red.p, 1024 * sizeof(double), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(dEdC, dG.p, nocc * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  tm.mark(-1);
   if ((rc = chk(cuda_check(ctx, cudaStreamSynchronize(s), "rijk_grad energy"))) || (rc = chk(check_device_error(ctx))))
     return rc;
   double es = 0.0, ec = 0.0;  // compensated: the 512 block sums, their compensations, then e_nuc
@@ -226,6 +262,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   neumaier_add(es, ec, e_nuc);
   *E = es + ec;
   if (!dEdI3 && !dEdPQ) {
+    tm.collect(ctx->stats);
     cleanup();
     return RIJK_OK;
   }
@@ -276,6 +313,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
       launch_xform_f64(static_cast<const double*>(ctx->B.p) + q0 * te, MOp, nq, nt, noccp, static_cast<double*>(Xc.p), s);
       X = static_cast<const double*>(Xc.p);
       ldx = nq * noccp;
+      tm.mark(1);
     } else {
       X = static_cast<const double*>(ctx->XT.p) + q0 * noccp;
       ldx = kdim;
@@ -296,9 +334,11 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
       g.C = pT, g.ldc = noccp, g.sC = npad * noccp;
       gemm_f64(g, nq, s);
     }
+    tm.mark(2);
     dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(nq));
     k_gamma_f64<<<grid, G_THREADS, gsmem, s>>>(pT, static_cast<const double*>(Ct.p), pD,
                                                static_cast<const double*>(ctx->w.p) + q0, n, npad, noccp, te, pGam);
+    tm.mark(3);
     if (dEdI3) {
       // dE/d(P|mu nu) += sum_{Q in chunk} Gamma^Q_{mu nu} M_QP, straight into the packed pair rows
       GemmF64Args g;
@@ -311,6 +351,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
       g.n_ao = n;
       gemm_f64(g, 1, s);
     }
+    tm.mark(4);
     if (dEdPQ) {
       // rows q0.. of G_QR = 1/2 sum_{mu nu} Gamma^Q B^R over the full squares: each stored element
       // of an off-diagonal tile once, of a diagonal tile one half
@@ -322,12 +363,11 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
       g.kdiag = 1;
       gemm_f64(g, 1, s);
     }
+    tm.mark(5);
   }
   release(Xc);
   release(Y);
   release(Tb);
-  if (dEdI3)
-    cudaMemcpyAsync(dEdI3, out.p, static_cast<size_t>(npair) * naux * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (dEdPQ) {
     // dE/dV = -M^T G M:  T1[Q][P'] = sum_R G[Q][R] M[R][P'];  out[P][P'] = -sum_Q M[Q][P] T1[Q][P']
     GemmF64Args g;
@@ -343,10 +383,14 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
     h.C = static_cast<double*>(Gm.p), h.ldc = naux;
     h.alpha = -1.0;
     gemm_f64(h, 1, s);
+    tm.mark(6);
     cudaMemcpyAsync(dEdPQ, Gm.p, static_cast<size_t>(naux) * naux * sizeof(double), cudaMemcpyDeviceToHost, s);
   }
+  if (dEdI3)
+    cudaMemcpyAsync(dEdI3, out.p, static_cast<size_t>(npair) * naux * sizeof(double), cudaMemcpyDeviceToHost, s);
   ctx->stats.grad_qchunk = qc;
   rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_grad");
+  if (!rc) tm.collect(ctx->stats);
   cleanup();
   (void)nt;
   return rc;

@@ -31,6 +31,9 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
 
 
+GRAD_STAGES = ("fock_energy_dEdC", "x_recompute", "y_t", "gamma", "d3c_M_gamma", "g_gamma_B", "dV_MtGM")
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("ms_setup_metric", ctypes.c_double), ("ms_setup_3c", ctypes.c_double),
                 ("ms_last_fock", ctypes.c_double), ("ms_coulomb", ctypes.c_double),
@@ -41,7 +44,8 @@ class Stats(ctypes.Structure):
                 ("profiled_stages", ctypes.c_int), ("ms_stage", ctypes.c_double * 12),
                 ("stage_names", (ctypes.c_char * 24) * 12), ("ms_setup_ints", ctypes.c_double),
                 ("kernels_setup_ints", ctypes.c_int), ("q0", ctypes.c_long), ("nq", ctypes.c_long),
-                ("grad_qchunk", ctypes.c_long)]
+                ("grad_qchunk", ctypes.c_long), ("ms_grad_stage", ctypes.c_double * 7),
+                ("ms_grad_total", ctypes.c_double)]
 
 
 class BasisT(ctypes.Structure):
@@ -365,7 +369,8 @@ class FockBuilder:
     def stats(self):
         s = Stats()
         self._check(lib().rijk_get_stats(self._h, ctypes.byref(s)))
-        out = {k: getattr(s, k) for k, _ in Stats._fields_ if k not in ("ms_stage", "stage_names")}
+        out = {k: getattr(s, k) for k, _ in Stats._fields_ if k not in ("ms_stage", "stage_names", "ms_grad_stage")}
+        out["grad_stages"] = dict(zip(GRAD_STAGES, list(s.ms_grad_stage)))
         k = s.profiled_stages
         out["stages"] = {s.stage_names[i].value.decode(): s.ms_stage[i] for i in range(k)}
         return out
