@@ -41,7 +41,11 @@ NCU_TRAFFIC = {("h2o16_dz", "xform_f64"): 1.277529e9 + 0.437618e9,
                ("h2o16_dz", "syrk_tc"): 0.228261e9 + 0.030061e9,
                ("h2o16_dz", "syrk_i8"): 0.970246e9 + 0.088795e9,
                ("h2o16_dz", "coulomb_w_mixed"): 0.639341e9 + 0.004234e9,
-               ("h2o16_dz", "coulomb_j_mixed"): 0.638610e9 + 0.010762e9}
+               ("h2o16_dz", "coulomb_j_mixed"): 0.638610e9 + 0.010762e9,
+               # (H2O)32 cc-pVTZ: the half-transform captured on a synthetic case with its orbital shape and
+               # 256 aux functions (4.892e9 read + 0.326e9 written per 80-orbital batch), scaled by aux
+               # functions (4448) and batches (2)
+               ("h2o32_tz", "xform_f64"): (4.892048e9 + 0.326164e9) / 256 * 4448 * 2}
 WORKLOAD_NAMES = {"h2o6_dz": "(H2O)6 cc-pVDZ/cc-pVDZ-JKFIT", "h2o16_dz": "(H2O)16 cc-pVDZ/cc-pVDZ-JKFIT",
                   "c40h82_dz": "C40H82 cc-pVDZ/cc-pVDZ-JKFIT", "h2o32_tz": "(H2O)32 cc-pVTZ/cc-pVTZ-JKFIT"}
 METRIC = "RI-JK Fock builds/s (FP64 drop-in; mixed and SCF time beside it)"
@@ -681,8 +685,9 @@ def main():
         achieved = amount / (stage_ms[top] * 1e-3) / 1e12
         roof = {"kernel": top, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak, "traffic": NCU_TRAFFIC.get((args.workload, top)),
-                "traffic_note": "bytes per launch from one ncu capture (profiles/); algorithmic: read B once, "
-                                "write XT once = %.3e" % (tile_elems * naux * 8.0 + npad * naux * noccp * 8.0),
+                "traffic_note": "DRAM bytes of the stage (all its launches) from ncu captures (profiles/); "
+                                "algorithmic: read B once, write XT once = %.3e" % (
+                                    tile_elems * naux * 8.0 + npad * naux * noccp * 8.0),
                 "peak_source": "FP64 DMMA: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)"}
     cw = stage_ms.get("coulomb_w", 0.0) + stage_ms.get("coulomb_j", 0.0)
     coul = {"achieved_gbs": 2 * tile_elems * naux * 8.0 / (cw * 1e-3) / 1e9 if cw else None, "peak_gbs": hbm}

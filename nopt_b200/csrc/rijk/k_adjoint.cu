@@ -368,6 +368,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   release(Xc);
   release(Y);
   release(Tb);
+  tm.mark(-1);  // the frees above wait on the host: that gap is not a stage
   if (dEdPQ) {
     // dE/dV = -M^T G M:  T1[Q][P'] = sum_R G[Q][R] M[R][P'];  out[P][P'] = -sum_Q M[Q][P] T1[Q][P']
     GemmF64Args g;

@@ -41,10 +41,11 @@ __device__ __forceinline__ void cp_async16n(void* smem, const void* gmem, int by
 }
 
 // One operand tile of 64 rows (m or n) x 32 k.  kmajor: global X[row * ld + k] staged [row][k]
-// (stride LDK); else global X[k * ld + row] staged [k][row] (stride LDM).
+// (stride LDK); else global X[k * ld + row] staged [k][row] (stride LDM).  `full`: every element of
+// the tile is in bounds, so the copies skip the per-pair checks.
 template <bool KMAJOR, bool VEC>
 __device__ __forceinline__ void load_tile(double* sm, const double* __restrict__ X, long ld, long rows, long K,
-                                          long r0, long k0, int tid) {
+                                          long r0, long k0, int tid, bool full) {
 #pragma unroll
   for (int it = 0; it < 8; ++it) {
     const int idx = tid + it * GM_THREADS;  // 1024 pairs of doubles
@@ -59,13 +60,22 @@ __device__ __forceinline__ void load_tile(double* sm, const double* __restrict__
     const long row = KMAJOR ? r0 + a : r0 + 2 * b;
     const long k = KMAJOR ? k0 + 2 * b : k0 + a;
     double* dst = KMAJOR ? sm + a * LDK + 2 * b : sm + a * LDM + 2 * b;
+    const double* src = X + (KMAJOR ? row * ld + k : k * ld + row);
+    if (full) {
+      if (VEC) {
+        cp_async16n(dst, src, 16);
+      } else {
+        cp_async8(dst, src, true);
+        cp_async8(dst + 1, src + 1, true);
+      }
+      continue;
+    }
     // valid doubles of the pair (the second runs along k for KMAJOR, along rows otherwise)
     int nv;
     if (KMAJOR)
       nv = row < rows ? static_cast<int>(min(2L, max(0L, K - k))) : 0;
     else
       nv = k < K ? static_cast<int>(min(2L, max(0L, rows - row))) : 0;
-    const double* src = X + (KMAJOR ? row * ld + k : k * ld + row);
     if (VEC) {
       cp_async16n(dst, nv > 0 ? src : X, nv * 8);
     } else {
@@ -97,34 +107,35 @@ __device__ __forceinline__ void warp_mma_chunk_ab(double (&acc)[4][4][2], const 
   }
 }
 
-__device__ __forceinline__ bool diag_tile(long e) {
-  long I, J;
-  tri_decode(e / TILE2, I, J);
-  return I == J;
-}
-
 template <bool AK, bool BK, bool VEC>
-__global__ void __launch_bounds__(GM_THREADS) k_gemm_f64(GemmF64Args p) {
+__global__ void __launch_bounds__(GM_THREADS) k_gemm_f64(GemmF64Args p, long ntn) {
   extern __shared__ __align__(16) double smem_gm[];
   double* sA[2] = {smem_gm, smem_gm + GM_STAGE};
   double* sB[2] = {smem_gm + 2 * GM_STAGE, smem_gm + 3 * GM_STAGE};
-  const long m0 = static_cast<long>(blockIdx.x) * 64, n0 = static_cast<long>(blockIdx.y) * 64;
-  const long bz = blockIdx.z;
+  // 1-D raster, N tiles fastest: the CTAs that share an A panel run together, so it is read from
+  // HBM once and the (smaller) B operand is served from L2
+  const long tile = blockIdx.x;
+  const long m0 = (tile / ntn) * 64, n0 = (tile % ntn) * 64;
+  const long bz = blockIdx.y;
   const double* A = p.A + bz * p.sA;
   const double* B = p.B + bz * p.sB;
   double* C = p.C + bz * p.sC;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
+  const bool mfull = m0 + 64 <= p.M, nfull = n0 + 64 <= p.N;
 
   auto load = [&](int stage, long k0) {
-    load_tile<AK, VEC>(sA[stage], A, p.lda, p.M, p.K, m0, k0, tid);
-    load_tile<BK, VEC>(sB[stage], B, p.ldb, p.N, p.K, n0, k0, tid);
+    const bool kfull = k0 + KC <= p.K;
+    load_tile<AK, VEC>(sA[stage], A, p.lda, p.M, p.K, m0, k0, tid, mfull && kfull);
+    load_tile<BK, VEC>(sB[stage], B, p.ldb, p.N, p.K, n0, k0, tid, nfull && kfull);
   };
   double acc[4][4][2];
   zero_acc(acc);
   const long nk = (p.K + KC - 1) / KC;
   load(0, 0);
   cp_async_commit();
+  long diag_t = -1;  // kdiag: the packed tile of the current chunk and its weight
+  double sc = 1.0;
   for (long kc = 0; kc < nk; ++kc) {
     if (kc + 1 < nk) {
       load(static_cast<int>((kc + 1) & 1), (kc + 1) * KC);
@@ -133,8 +144,13 @@ __global__ void __launch_bounds__(GM_THREADS) k_gemm_f64(GemmF64Args p) {
     } else {
       cp_async_wait<0>();
     }
+    if (p.kdiag && (kc * KC) / TILE2 != diag_t) {  // a 32-chunk lies inside one 64 x 64 tile
+      diag_t = (kc * KC) / TILE2;
+      long I, J;
+      tri_decode(diag_t, I, J);
+      sc = I == J ? 0.5 : 1.0;
+    }
     __syncthreads();
-    const double sc = (p.kdiag && diag_tile(kc * KC)) ? 0.5 : 1.0;  // a 32-chunk lies inside one tile
     warp_mma_chunk_ab<AK, BK>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * 32, lane, sc);
     __syncthreads();
   }
@@ -190,8 +206,9 @@ template <bool AK, bool BK, bool VEC>
 void launch_one(const GemmF64Args& p, long batch, cudaStream_t s) {
   const size_t smem = 4 * GM_STAGE * sizeof(double);
   ensure_smem_limit(reinterpret_cast<const void*>(k_gemm_f64<AK, BK, VEC>), smem);
-  dim3 grid(static_cast<unsigned>((p.M + 63) / 64), static_cast<unsigned>((p.N + 63) / 64), static_cast<unsigned>(batch));
-  k_gemm_f64<AK, BK, VEC><<<grid, GM_THREADS, smem, s>>>(p);
+  const long ntm = (p.M + 63) / 64, ntn = (p.N + 63) / 64;
+  dim3 grid(static_cast<unsigned>(ntm * ntn), static_cast<unsigned>(batch));
+  k_gemm_f64<AK, BK, VEC><<<grid, GM_THREADS, smem, s>>>(p, ntn);
 }
 
 bool aligned16(const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; }
@@ -200,6 +217,7 @@ bool aligned16(const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 
 
 void gemm_f64(const GemmF64Args& p, long batch, cudaStream_t s) {
   if (p.M <= 0 || p.N <= 0 || batch <= 0) return;
+  // grid limits: 2^31 - 1 tiles along x, 65535 batches along y (the callers stay far below both)
   // 16-byte copies need every row of both operands (and every batch) to start 16-byte aligned
   const bool vec = aligned16(p.A) && aligned16(p.B) && p.lda % 2 == 0 && p.ldb % 2 == 0 &&
                    (batch == 1 || (p.sA % 2 == 0 && p.sB % 2 == 0));
