@@ -337,14 +337,18 @@ def cpu_baseline_for(si, DM, MO, workload, seed, nslices, budget_s):
 def grad_report(fb, si, MOc, nocc, fp64_peak, reps=3):
     """rijk_grad (E, dE/dC, dE/d(P|mu nu) packed, dE/d(P|Q); host outputs): wall time per call, and
     the device time, FLOPs and FP64 roofline fraction of each stage (profiling events)."""
-    from nopt_b200 import rijk
-    fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)  # first call: module loads
+    # outputs allocated once and reused, as a caller keeps its gradient arrays between calls (new
+    # arrays would put the first-touch page faults of GBs of host memory into every call)
+    out3 = np.empty((si.n * (si.n + 1) // 2, si.naux))
+    outV = np.empty((si.naux, si.naux))
+    kw = dict(want_3c=True, want_metric=True, out3=out3, outV=outV)
+    fb.grad(MOc, nocc, si.H, si.Enuc, **kw)  # first call: module loads, first touch of the outputs
     t0 = time.perf_counter()
     for _ in range(reps):
-        fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
+        fb.grad(MOc, nocc, si.H, si.Enuc, **kw)
     wall = (time.perf_counter() - t0) / reps
     fb.set_profiling(True)
-    fb.grad(MOc, nocc, si.H, si.Enuc, want_3c=True, want_metric=True)
+    fb.grad(MOc, nocc, si.H, si.Enuc, **kw)
     fb.set_profiling(False)
     st = fb.stats()
     n, naux = si.n, si.naux
@@ -368,11 +372,12 @@ def grad_report(fb, si, MOc, nocc, fp64_peak, reps=3):
             "flops": sum(flops.values()), "fp64_peak_tflops": fp64_peak,
             "what": "rijk_grad through the C ABI: E, dE/dC, dE/d(P|mu nu) (packed) and dE/d(P|Q) to host memory; "
                     "device_ms = its kernels before the host copies (stage events), wall_ms includes the copies "
-                    "(%.2f GB) and the call's buffer allocation" % ((n * (n + 1) // 2 * naux + naux * naux) * 8 / 1e9)}
+                    "(%.2f GB, into pageable arrays reused between calls) and the call's device buffer allocation"
+                    % ((n * (n + 1) // 2 * naux + naux * naux) * 8 / 1e9)}
 
 
 def c40h82_grad(seed, dev, fp64_peak, chunk=1200):
-    """BASELINE's C40H82 adjoint case: mixed -> FP64 SCF, then rijk_grad with Gamma in aux chunks and
+    """The C40H82 cc-pVDZ adjoint case: mixed -> FP64 SCF, then rijk_grad with Gamma in aux chunks and
     X^Q recomputed in tiles (the path taken when HBM cannot hold Gamma for every aux function)."""
     from nopt_b200 import rijk
     si, _, _ = build_system("c40h82_dz", seed, ri_integrals=False)

@@ -335,14 +335,19 @@ class FockBuilder:
         """Aux functions per chunk of grad's Gamma stage (0: automatic, from free HBM)."""
         self._check(lib().rijk_set_grad_chunk(self._h, int(q_per_chunk)))
 
-    def grad(self, MO, n_c, H, e_nuc, want_3c=False, want_metric=False):
-        """(E, dE/dMO (n_c x n), dE/d(P|mu nu) packed [pair][P] or None, dE/d(P|Q) or None)."""
+    def grad(self, MO, n_c, H, e_nuc, want_3c=False, want_metric=False, out3=None, outV=None):
+        """(E, dE/dMO (n_c x n), dE/d(P|mu nu) packed [pair][P] or None, dE/d(P|Q) or None).  out3 / outV
+        (C-contiguous float64 arrays of those shapes) receive the last two instead of new arrays."""
         n = self.n
         MO = _c(MO[:n_c])
         E = ctypes.c_double(0.0)
         dC = np.empty((n_c, n))
-        d3 = np.empty((n * (n + 1) // 2, self.naux)) if want_3c else None
-        dV = np.empty((self.naux, self.naux)) if want_metric else None
+        shape3, shapeV = (n * (n + 1) // 2, self.naux), (self.naux, self.naux)
+        for o, sh in ((out3, shape3), (outV, shapeV)):
+            if o is not None and (o.shape != sh or o.dtype != np.float64 or not o.flags.c_contiguous):
+                raise ValueError("grad output array must be C-contiguous float64 of shape %s" % (sh,))
+        d3 = (out3 if out3 is not None else np.empty(shape3)) if want_3c else None
+        dV = (outV if outV is not None else np.empty(shapeV)) if want_metric else None
         self._check(lib().rijk_grad(self._h, _p(MO), int(n_c), _p(_c(H)), float(e_nuc), ctypes.byref(E), _p(dC),
                                     _p(d3), _p(dV)))
         return E.value, dC, d3, dV
