@@ -132,8 +132,10 @@ __global__ void __launch_bounds__(GM_THREADS) k_gemm_f64(GemmF64Args p, long ntn
   double acc[4][4][2];
   zero_acc(acc);
   const long nk = (p.K + KC - 1) / KC;
-  load(0, 0);
-  cp_async_commit();
+  if (nk > 0) {  // K = 0 leaves acc at zero and issues no copy
+    load(0, 0);
+    cp_async_commit();
+  }
   long diag_t = -1;  // kdiag: the packed tile of the current chunk and its weight
   double sc = 1.0;
   for (long kc = 0; kc < nk; ++kc) {

@@ -242,3 +242,30 @@ def test_grad_c40h82_after_mixed_scf_recompute_path():
     assert _rel(dCc, dC) < 1e-12 and _rel(dVc, dV) < 1e-11
     g = dC @ MO[nocc:r["nmo"]].T  # 4 F_ai = (4 C_occ F) C_vir^T
     assert float(np.max(np.abs(g))) < 1e-6, float(np.max(np.abs(g)))
+
+
+@pytest.mark.parametrize("n,naux,nocc,chunk", [(131, 75, 13, 0), (65, 33, 1, 0), (131, 75, 13, 29), (200, 97, 37, 41)])
+def test_grad_ragged_random_matches_closed_form(n, naux, nocc, chunk):
+    """Odd n, naux and n_c (8-byte copies and ragged tiles in the DMMA GEMMs, the pair epilogue's edge
+    rows), and aux chunks of odd size (contractions of K = 29 or 41 over the chunk)."""
+    rng = np.random.default_rng(n + naux)
+    A = rng.normal(size=(naux, naux))
+    V = A @ A.T / naux + np.eye(naux)
+    I3 = rng.normal(size=(n * (n + 1) // 2, naux)) * 0.1
+    Hm = rng.normal(size=(n, n))
+    H = (Hm + Hm.T) / np.sqrt(n)
+    C, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    MO = C.T.copy()
+    M = O.s05_calc(V)[0]
+    Er, dCr, d3r, dVr = O.adjoint_reference(I3, M, H, MO, nocc, 0.7)
+    with rijk.FockBuilder(0) as fb:
+        fb.set_metric(V)
+        fb.set_3c(I3, n)
+        if chunk:
+            fb.set_grad_chunk(chunk)
+        E, dC, d3, dV = fb.grad(MO, nocc, H, 0.7, want_3c=True, want_metric=True)
+        assert fb.stats()["grad_qchunk"] == (chunk or naux)
+    assert abs(E - Er) < 1e-9 * max(1.0, abs(Er))
+    assert np.max(np.abs(dC - dCr)) < 1e-9 * max(1.0, np.max(np.abs(dCr)))
+    assert np.max(np.abs(d3 - d3r)) < 1e-9 * max(1.0, np.max(np.abs(d3r)))
+    assert np.max(np.abs(dV - dVr)) < 1e-9 * max(1.0, np.max(np.abs(dVr)))
