@@ -559,14 +559,13 @@ def main():
 
     dD = torch.from_numpy(DM).to(dev)
     dMO = torch.from_numpy(MO[:nocc].copy()).to(dev)
-    dJ = torch.empty((n, n), dtype=torch.float64, device=dev)
-    dK = torch.empty((n, n), dtype=torch.float64, device=dev)
+    dJK = torch.empty((2, n, n), dtype=torch.float64, device=dev)  # J and K in one buffer: one collective
+    dJ, dK = dJK[0], dJK[1]
 
     def build(prec):
         fb.fock_device(dD.data_ptr(), dMO.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec)
         if sharded:  # partial J, K of this rank's aux slice -> full J, K (NCCL on the same stream)
-            dist.all_reduce(dJ)
-            dist.all_reduce(dK)
+            dist.all_reduce(dJK)
 
     def timed(prec, steps, warm):
         for _ in range(warm):
@@ -856,7 +855,7 @@ def main():
                          "ms_final: after the last iteration, closing build and orbitals)" % reps)
         scf = out
     fb.close()
-    del dD, dMO, dJ, dK
+    del dD, dMO, dJ, dK, dJK
     torch.cuda.empty_cache()
 
     cpu = None

@@ -53,12 +53,28 @@ class ShardedFockBuilder:
         self._allreduce(dJ, dK)
 
     def dm_to_f_transform_ri(self, DM, MO, n_c, precision=0):
-        """Host arrays in and out (the drop-in semantics of DM_to_F_transform_RI)."""
+        """Host arrays in and out (the drop-in semantics of DM_to_F_transform_RI).  Over NCCL: D and
+        the orbitals go up once, the partial build writes J and K into one device buffer, one
+        all-reduce sums it across the ranks, and J and K come down once -- the host traffic of a
+        one-GPU rijk_fock.  Over gloo (CPU ranks) the local builder's host J and K are summed."""
         import torch
-        J, K = self.local.dm_to_f_transform_ri(DM, MO, n_c, precision)
         backend = self.dist.get_backend(self.group)
-        dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
-        tJ = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
-        tK = torch.from_numpy(np.ascontiguousarray(K)).to(dev)
-        self._allreduce(tJ, tK)
-        return tJ.cpu().numpy(), tK.cpu().numpy()
+        if backend != "nccl":
+            J, K = self.local.dm_to_f_transform_ri(DM, MO, n_c, precision)
+            tJ = torch.from_numpy(np.ascontiguousarray(J))
+            tK = torch.from_numpy(np.ascontiguousarray(K))
+            self._allreduce(tJ, tK)
+            return tJ.numpy(), tK.numpy()
+        n = self.n
+        dev = torch.device("cuda", torch.cuda.current_device())
+        stream = torch.cuda.current_stream(dev)
+        self.local.set_stream(stream.cuda_stream)  # the build and the collective on one stream
+        dD = torch.from_numpy(np.ascontiguousarray(DM, dtype=np.float64)).to(dev)
+        rows = max(int(n_c), 1)
+        MOh = np.ascontiguousarray(MO[:rows], dtype=np.float64) if n_c > 0 else np.zeros((1, n))
+        dMO = torch.from_numpy(MOh).to(dev)
+        jk = torch.empty((2, n, n), dtype=torch.float64, device=dev)
+        self.local.fock_device(dD.data_ptr(), dMO.data_ptr(), n_c, jk[0].data_ptr(), jk[1].data_ptr(), precision)
+        self._allreduce(jk)
+        out = jk.cpu().numpy()
+        return out[0], out[1]

@@ -49,3 +49,37 @@ def test_two_aux_slices_sum_to_full():
         with pytest.raises(rijk.RijkError) as e:
             fb.scf(si.H, si.S, si.nocc, si.Enuc)
         assert e.value.code == rijk.ERR_STATE
+
+
+def test_sharded_builder_nccl_device_path_one_rank():
+    """The NCCL path of ShardedFockBuilder.dm_to_f_transform_ri (D and the orbitals up once, the
+    partial build into one device buffer, one all-reduce, J and K down once) in a one-rank NCCL
+    group on this GPU, against the plain builder."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    from nopt_b200.parallel import ShardedFockBuilder
+    si = ints.SystemIntegrals(water_cluster((2, 3), seed=0), "cc-pvdz", "cc-pvdz-jkfit")
+    rng = np.random.default_rng(9)
+    C, _ = np.linalg.qr(rng.normal(size=(si.n, si.n)))
+    MO = C.T.copy()
+    DM = O.gen_hf_dm(MO, si.n, si.nocc)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        with rijk.FockBuilder(0) as fb, rijk.FockBuilder(0) as ref:
+            sb = ShardedFockBuilder(fb)
+            sb.setup(si.V, si.I3, si.n)
+            assert sb.slice == (0, si.naux)
+            J, K = sb.dm_to_f_transform_ri(DM, MO, si.nocc)
+            ref.set_metric(si.V)
+            ref.set_3c(si.I3, si.n)
+            Jr, Kr = ref.dm_to_f_transform_ri(DM, MO, si.nocc)
+        assert np.max(np.abs(J - Jr)) < 1e-12 and np.max(np.abs(K - Kr)) < 1e-12
+    finally:
+        dist.destroy_process_group()
