@@ -6,6 +6,7 @@
  *   rijk_set_3c       replaces the RI_AA set-up of gen_RI_AA / regen_RI_AA
  *                                                          src/RI.cpp:34-101 (consumer of calc_2el_AO_INTS_RI,
  *                                                          src/libint_link.cpp:2261-2350)
+ *   rijk_begin_3c, rijk_add_3c_block  the same, fed block by block from that shell loop
  *   rijk_set_basis    replaces gen_RI_AA whole, integrals included  src/RI.cpp:34-79
  *   rijk_eri2c        replaces RI_V_calc                            src/libint_link.cpp:2049-2107
  *   rijk_eri3c        replaces calc_2el_AO_INTS_RI                  src/libint_link.cpp:2261-2350
@@ -112,6 +113,20 @@ int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1);
 /* Three-centre integrals (host array, layout RIJK_LAYOUT_*).  Forms the fitted tensor
  * B^Q_{mu nu} = sum_P M_QP (P|mu nu) on the GPU, stored packed (mu >= nu) in HBM. */
 int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n_ao, long naux, int layout);
+
+/* The same fitted tensor from three-centre integrals handed over in blocks of orbital rows, for
+ * callers whose (mu nu|P) does not fit in host memory at once (the reference's RI_AA is n^2 naux
+ * doubles, 123 GB at (H2O)32 cc-pVTZ; it is filled by calc_2el_AO_INTS_RI's shell loop,
+ * src/libint_link.cpp:2261-2350).  rijk_begin_3c starts one (after rijk_set_metric and any
+ * rijk_set_aux_range); rijk_add_3c_block then takes the rows mu in [mu0, mu1) of the layout, the
+ * ranges consecutive from mu0 = 0 and each block usable again by the caller when the call returns:
+ *   RIJK_LAYOUT_NOPT_FULL  block[((mu - mu0) n_ao + nu) naux + P]
+ *   RIJK_LAYOUT_PACKED     block[(mu (mu + 1) / 2 + nu - mu0 (mu0 + 1) / 2) naux + P], nu <= mu
+ * Whole 64-row tile rows are contracted with the metric factor as they complete; the block that ends
+ * at n_ao completes the fitted tensor, bit-identical to rijk_set_3c's.  An error, rijk_set_metric,
+ * rijk_set_aux_range or rijk_set_3c abandons the stream (the context then has no fitted tensor). */
+int rijk_begin_3c(rijk_ctx* ctx, long n_ao, long naux, int layout);
+int rijk_add_3c_block(rijk_ctx* ctx, long mu0, long mu1, const double* block);
 
 /* A contracted Gaussian basis as shell arrays, in the order of a basis-set file.  Coefficients
  * are as printed there; the library normalises them as libint does (x^l primitive

@@ -34,6 +34,7 @@ CUDA_SOURCES = [
     "rijk/rijk_cache.cu",
     "rijk/rijk_selftest.cu",
     "rijk/k_gemm.cu",
+    "rijk/rijk_stream3c.cu",
 ]
 
 

@@ -300,7 +300,8 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // before any buffer it may touch is freed
   DeviceBuf* bufs[] = {&ctx->M,  &ctx->B,     &ctx->Bmix,  &ctx->stageD, &ctx->stageMO, &ctx->stageJ,
                        &ctx->stageK, &ctx->Dt, &ctx->w,     &ctx->Jpart, &ctx->MOp,    &ctx->XT,
-                       &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab, &ctx->Xs, &ctx->Xe};
+                       &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab, &ctx->Xs, &ctx->Xe,
+                       &ctx->s3.raw};
   for (DeviceBuf* b : bufs) release(*b);
   for (DeviceBuf& b : ctx->scf) release(b);
   if (ctx->cublas) cublasDestroy(ctx->cublas);
@@ -360,6 +361,8 @@ RIJK_API int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1) {
   if (!ctx->have_metric) return set_err(ctx, RIJK_ERR_STATE, "rijk_set_aux_range: call rijk_set_metric first");
   if (q0 < 0 || q1 <= q0 || q1 > ctx->naux)
     return set_err(ctx, RIJK_ERR_ARG, "rijk_set_aux_range: [%ld, %ld) not inside [0, %ld)", q0, q1, ctx->naux);
+  cudaSetDevice(ctx->device);
+  stream3c_cancel(ctx);
   ctx->q0 = q0;
   ctx->nq = q1 - q0;
   ctx->have_b = false;
@@ -378,6 +381,8 @@ int set_metric_impl(rijk_ctx* ctx, const double* PQ, cudaMemcpyKind kind, long n
   if (naux > 65535) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_metric: naux = %ld exceeds 65535", naux);
   if (form != RIJK_METRIC_INVSQRT && form != RIJK_METRIC_CHOLESKY)
     return set_err(ctx, RIJK_ERR_ARG, "rijk_set_metric: unknown metric form %d", form);
+  cudaSetDevice(ctx->device);
+  stream3c_cancel(ctx);  // a new metric ends any streaming three-centre input in progress
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   const long nauxp = round_up(naux, KC);
@@ -494,6 +499,25 @@ RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int
 }
 
 namespace rijk {
+long rows_per_chunk(long n, long nauxp, int layout) {
+  const long npad = round_up(n, TILE), nt = npad / TILE;
+  const double budget = 2.0 * 1024 * 1024 * 1024;
+  const long rows = std::max<long>(1, static_cast<long>(budget / (static_cast<double>(TILE) *
+                                                                  (layout == RIJK_LAYOUT_NOPT_FULL ? n : npad) *
+                                                                  nauxp * 8.0)));
+  return std::min(rows, nt);
+}
+
+void pair_rows(int layout, long n, long mu0, long mu1, long* first, long* count) {
+  if (layout == RIJK_LAYOUT_NOPT_FULL) {
+    *first = mu0 * n;
+    *count = (mu1 - mu0) * n;
+  } else {
+    *first = mu0 * (mu0 + 1) / 2;
+    *count = mu1 * (mu1 + 1) / 2 - *first;
+  }
+}
+
 int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& fill) {
   if (n <= 0 || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_3c: bad sizes");
   if (layout != RIJK_LAYOUT_NOPT_FULL && layout != RIJK_LAYOUT_PACKED)
@@ -502,6 +526,7 @@ int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& f
   if (naux != ctx->naux)
     return set_err(ctx, RIJK_ERR_ARG, "rijk_set_3c: naux %ld differs from the metric's %ld", naux, ctx->naux);
   cudaSetDevice(ctx->device);
+  stream3c_cancel(ctx);
   cudaStream_t s = ctx->stream;
   const long npad = round_up(n, TILE), nt = npad / TILE, ntile = nt * (nt + 1) / 2;
   const long nauxp = round_up(naux, KC);
@@ -513,19 +538,9 @@ int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& f
   if ((rc = ensure(ctx, ctx->B, static_cast<size_t>(nq) * ntile * TILE2 * sizeof(double), "fitted tensor B")))
     return rc;
   // Raw integrals come in blocks of whole tile rows, at most ~2 GiB each.
-  const double budget = 2.0 * 1024 * 1024 * 1024;
-  long rows_per = std::max<long>(1, static_cast<long>(budget / (static_cast<double>(TILE) *
-                                                               (layout == RIJK_LAYOUT_NOPT_FULL ? n : npad) * nauxp * 8.0)));
-  rows_per = std::min(rows_per, nt);
+  const long rows_per = rows_per_chunk(n, nauxp, layout);
   auto pairs_of = [&](long I0, long I1, long& first, long& count) {
-    long mu0 = I0 * TILE, mu1 = std::min(I1 * TILE, n);
-    if (layout == RIJK_LAYOUT_NOPT_FULL) {
-      first = mu0 * n;
-      count = (mu1 - mu0) * n;
-    } else {
-      first = mu0 * (mu0 + 1) / 2;
-      count = mu1 * (mu1 + 1) / 2 - first;
-    }
+    pair_rows(layout, n, I0 * TILE, std::min(I1 * TILE, n), &first, &count);
   };
   long maxcount = 0;
   for (long I0 = 0; I0 < nt; I0 += rows_per) {

@@ -80,6 +80,17 @@ struct rijk_ctx {
   rijk::DeviceBuf Xe;       // their row exponents, parts x npad2
   rijk::DeviceBuf scf[32];  // rijk_scf's work buffers, kept between calls
   double* noalloc_scratch = nullptr;  // device address of rijk_coulomb_noalloc's fixed scratch on `device`
+  // streaming three-centre input (rijk_begin_3c / rijk_add_3c_block) in progress
+  struct {
+    bool active = false;
+    long n = 0, naux = 0;
+    int layout = 0;
+    long rows_per = 0;  // tile rows per metric-contraction chunk
+    long next_mu = 0;   // first orbital row the next block must start at
+    long chunk_I0 = 0;  // tile rows [chunk_I0, chunk_I0 + rows_per) fill the staging buffer
+    double ms = 0.0;
+    rijk::DeviceBuf raw;
+  } s3;
 
   rijk_stats_t stats{};
   std::string last_error;
@@ -121,6 +132,12 @@ int set_metric_impl(rijk_ctx* ctx, const double* PQ, cudaMemcpyKind kind, long n
 // naux) into the device buffer raw.
 using ChunkFill = std::function<int(long mu0, long mu1, long first, long count, double* raw, long ld)>;
 int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& fill);
+// Tile rows per metric-contraction chunk (raw blocks of at most ~2 GiB) and the pair rows of orbital
+// rows [mu0, mu1) in a layout: first pair row and count.
+long rows_per_chunk(long n, long nauxp, int layout);
+void pair_rows(int layout, long n, long mu0, long mu1, long* first, long* count);
+// Abandons a streaming three-centre input in progress (rijk_add_3c_block), freeing its staging.
+void stream3c_cancel(rijk_ctx* ctx);
 
 // ---- rijk_noalloc.cu
 // Looks up the device address of rijk_coulomb_noalloc's fixed scratch array on ctx->device (which

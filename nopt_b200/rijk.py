@@ -110,6 +110,8 @@ def lib():
         L.rijk_set_metric.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_int]
         L.rijk_set_aux_range.argtypes = [_vp, ctypes.c_long, ctypes.c_long]
         L.rijk_set_3c.argtypes = [_vp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_int]
+        L.rijk_begin_3c.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_int]
+        L.rijk_add_3c_block.argtypes = [_vp, ctypes.c_long, ctypes.c_long, _dp]
         L.rijk_eri2c.argtypes = [_vp, P(BasisT), _dp]
         L.rijk_eri3c.argtypes = [_vp, P(BasisT), P(BasisT), ctypes.c_int, _dp]
         L.rijk_set_basis.argtypes = [_vp, P(BasisT), P(BasisT), ctypes.c_int, ctypes.c_long, ctypes.c_long]
@@ -196,6 +198,26 @@ class FockBuilder:
         I3 = _c(I3)
         self._check(lib().rijk_set_3c(self._h, _p(I3), int(n), I3.shape[-1], layout))
         self.n = n
+
+    def begin_3c(self, n, naux, layout=LAYOUT_PACKED):
+        """Start a streaming three-centre input (rijk_begin_3c)."""
+        self._check(lib().rijk_begin_3c(self._h, int(n), int(naux), layout))
+        self.n, self._s3 = n, (n, naux, layout)
+
+    def add_3c_block(self, mu0, mu1, block):
+        """Rows mu in [mu0, mu1) of the three-centre integrals in the layout given to begin_3c."""
+        self._check(lib().rijk_add_3c_block(self._h, int(mu0), int(mu1), _p(_c(block))))
+
+    def set_3c_streamed(self, I3, n, bounds, layout=LAYOUT_PACKED):
+        """The fitted tensor from I3 handed over in the orbital-row ranges `bounds` ([(mu0, mu1), ...])."""
+        naux = I3.shape[1]
+        self.begin_3c(n, naux, layout)
+        for mu0, mu1 in bounds:
+            if layout == LAYOUT_NOPT_FULL:
+                r0, r1 = mu0 * n, mu1 * n
+            else:
+                r0, r1 = mu0 * (mu0 + 1) // 2, mu1 * (mu1 + 1) // 2
+            self.add_3c_block(mu0, mu1, I3[r0:r1])
 
     def set_basis(self, orb, aux, metric_form=METRIC_INVSQRT, q0=0, q1=0):
         """gen_RI_AA on the GPU: integrals, metric factor and fitted tensor from two Basis objects."""
