@@ -175,7 +175,7 @@ def test_grad_water16_converged_matches_oracle_and_recompute(water16):
     # (cuSOLVER) and the oracle (LAPACK) form independently; at naux = 1856 its conditioning puts
     # their agreement near 1e-9 relative, hence 1e-8 for these two
     assert _rel(dC, dCr) < 1e-9 and _rel(d3, d3r) < 1e-8 and _rel(dV, dVr) < 1e-8
-    # chunked G rows come from DGEMMs of another shape (another summation order)
+    # chunked G rows come from GEMMs over other aux chunks (another summation order)
     assert _rel(dCc, dC) < 1e-12 and _rel(d3c, d3) < 1e-11 and _rel(dVc, dV) < 1e-11
     # converged: the occupied-virtual block of 4 F (the SCF's rotation gradient) vanishes
     g = dC @ MO[si.nocc:].T  # 4 F_ai = (4 C_occ F) C_vir^T
