@@ -19,10 +19,13 @@ namespace rijk {
 
 constexpr int X_THREADS = 128;
 
+// Grid (nb * nt, naux): block x = J nb + b handles orbital batch b (rows i0 + b NOCCP of MOp) of tile
+// column J, so the nb batches of one (J, Q) run back to back and the later ones read the tiles of B^Q
+// from L2.
 template <int NF>
 __global__ void __launch_bounds__(X_THREADS)
-    k_xform_f64(const double* __restrict__ B, const double* __restrict__ MOp, long nt, long npad, long tile_elems,
-                long kdim, long noccp_total, long i0, double* __restrict__ XT) {
+    k_xform_f64(const double* __restrict__ B, const double* __restrict__ MOp_all, long nt, long npad, long tile_elems,
+                long kdim, long noccp_total, long i0_first, int nb, double* __restrict__ XT) {
   constexpr int NOCCP = NF * 16;
   constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
   constexpr int B_STAGE = NOCCP * LDK;
@@ -30,7 +33,9 @@ __global__ void __launch_bounds__(X_THREADS)
   double* sA[2] = {smem, smem + A_STAGE};
   double* sB[2] = {smem + 2 * A_STAGE, smem + 2 * A_STAGE + B_STAGE};
 
-  const long J = blockIdx.x;
+  const long J = blockIdx.x / nb;
+  const long i0 = i0_first + static_cast<long>(blockIdx.x % nb) * NOCCP;
+  const double* MOp = MOp_all + i0 * npad;
   const long Q = blockIdx.y;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -95,9 +100,9 @@ __global__ void __launch_bounds__(X_THREADS)
   }
 }
 
-// One orbital batch: rows i0 .. i0 + NF*16 of MOp into columns Q*noccp_total + i0 + ... of XT.
+// nb orbital batches of NF*16 rows from row i0 of MOp into columns Q*noccp_total + i0 + ... of XT.
 template <int NF>
-static void launch_xform_nf(const double* B, const double* MOp, long naux, long nt, long noccp_total, long i0,
+static void launch_xform_nf(const double* B, const double* MOp, long naux, long nt, long noccp_total, long i0, int nb,
                             double* XT, cudaStream_t s) {
   constexpr int NOCCP = NF * 16;
   constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
@@ -105,27 +110,33 @@ static void launch_xform_nf(const double* B, const double* MOp, long naux, long 
   ensure_smem_limit(reinterpret_cast<const void*>(k_xform_f64<NF>), smem);
   long npad = nt * TILE;
   long tile_elems = nt * (nt + 1) / 2 * TILE2;
-  dim3 grid(static_cast<unsigned>(nt), static_cast<unsigned>(naux));
-  k_xform_f64<NF><<<grid, X_THREADS, smem, s>>>(B, MOp + i0 * npad, nt, npad, tile_elems, naux * noccp_total,
-                                                 noccp_total, i0, XT);
+  dim3 grid(static_cast<unsigned>(nt * nb), static_cast<unsigned>(naux));
+  k_xform_f64<NF><<<grid, X_THREADS, smem, s>>>(B, MOp, nt, npad, tile_elems, naux * noccp_total, noccp_total, i0, nb,
+                                                 XT);
 }
 
-// The orbitals go in batches of at most 96 (NF <= 6 keeps the accumulators in registers).
-void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s) {
-  const long nb = (noccp + 95) / 96;
-  const long per = round_up((noccp + nb - 1) / nb, 16);
-  for (long i0 = 0; i0 < noccp; i0 += per) {
-    const long cnt = (noccp - i0 < per) ? noccp - i0 : per;
-    switch (cnt / 16) {
-      case 1: launch_xform_nf<1>(B, MOp, naux, nt, noccp, i0, XT, s); break;
-      case 2: launch_xform_nf<2>(B, MOp, naux, nt, noccp, i0, XT, s); break;
-      case 3: launch_xform_nf<3>(B, MOp, naux, nt, noccp, i0, XT, s); break;
-      case 4: launch_xform_nf<4>(B, MOp, naux, nt, noccp, i0, XT, s); break;
-      case 5: launch_xform_nf<5>(B, MOp, naux, nt, noccp, i0, XT, s); break;
-      case 6: launch_xform_nf<6>(B, MOp, naux, nt, noccp, i0, XT, s); break;
-      default: break;
-    }
+static void launch_xform_batches(int nf, const double* B, const double* MOp, long naux, long nt, long noccp, long i0,
+                                 int nb, double* XT, cudaStream_t s) {
+  switch (nf) {
+    case 1: launch_xform_nf<1>(B, MOp, naux, nt, noccp, i0, nb, XT, s); break;
+    case 2: launch_xform_nf<2>(B, MOp, naux, nt, noccp, i0, nb, XT, s); break;
+    case 3: launch_xform_nf<3>(B, MOp, naux, nt, noccp, i0, nb, XT, s); break;
+    case 4: launch_xform_nf<4>(B, MOp, naux, nt, noccp, i0, nb, XT, s); break;
+    case 5: launch_xform_nf<5>(B, MOp, naux, nt, noccp, i0, nb, XT, s); break;
+    case 6: launch_xform_nf<6>(B, MOp, naux, nt, noccp, i0, nb, XT, s); break;
+    default: break;
   }
+}
+
+// The orbitals go in batches of at most 96 (NF <= 6 keeps the accumulators in registers).  The
+// full-size batches run in one launch (each tile column's batches back to back, B^Q read once from
+// HBM); a smaller last batch gets a launch of its own.
+void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s) {
+  const long nbatch = (noccp + 95) / 96;
+  const long per = round_up((noccp + nbatch - 1) / nbatch, 16);
+  const long nfull = noccp / per, rest = noccp - nfull * per;
+  if (nfull > 0) launch_xform_batches(static_cast<int>(per / 16), B, MOp, naux, nt, noccp, 0, static_cast<int>(nfull), XT, s);
+  if (rest > 0) launch_xform_batches(static_cast<int>(rest / 16), B, MOp, naux, nt, noccp, nfull * per, 1, XT, s);
 }
 
 constexpr int S_THREADS = 128;
