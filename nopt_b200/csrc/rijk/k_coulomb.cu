@@ -110,6 +110,13 @@ void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_el
   k_coulomb_w<<<grid, W_THREADS, 0, s>>>(B, Dt, naux, tile_elems, w);
 }
 
+cudaError_t preload_coulomb_kernels() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k_coulomb_w);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_coulomb_j);
+  return e;
+}
+
 void launch_coulomb_j(const double* B, const double* w, long naux, long tile_elems, int nsplit, double* Jpart,
                       cudaStream_t s) {
   long qper = (naux + nsplit - 1) / nsplit;

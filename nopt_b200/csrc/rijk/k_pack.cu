@@ -125,6 +125,14 @@ void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt
   k_pack_density<<<static_cast<unsigned>(ntile), 256, 0, s>>>(D, n, npad, Dt);
 }
 
+cudaError_t preload_density_kernels() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k_pack_density);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_sum_splits<double>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_unpack_blocks);
+  return e;
+}
+
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s) {
   k_pack_mo<<<grid_for(noccp * npad, 256), 256, 0, s>>>(MO, nocc, n, noccp, npad, MOp);
 }

@@ -141,8 +141,9 @@ void stream3c_cancel(rijk_ctx* ctx);
 
 // ---- rijk_noalloc.cu
 // Looks up the device address of rijk_coulomb_noalloc's fixed scratch array on ctx->device (which
-// must be current) into ctx->noalloc_scratch.  The lookup loads the module holding the array, and
-// with it the array itself, so rijk_create does it while allocating is still allowed.
+// must be current) into ctx->noalloc_scratch, and loads the modules of the kernels that call launches.
+// The lookup loads the module holding the array, and with it the array itself; a module load is a
+// device allocation too.  rijk_create does both while allocating is still allowed.
 int noalloc_resolve(rijk_ctx* ctx);
 
 // ---- k_gemm.cu
@@ -168,6 +169,9 @@ struct GemmF64Args {
 void gemm_f64(const GemmF64Args& p, long batch, cudaStream_t s);
 
 // ---- k_pack.cu
+// Loads (CUDA loads modules lazily, on a kernel's first use) the density packing and symmetric unpacking
+// kernels on the current device.
+cudaError_t preload_density_kernels();
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s);
 void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s);
@@ -182,6 +186,8 @@ void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const
                                   long naux, long nt, long I0, long I1, double* B, cudaStream_t s);
 
 // ---- k_coulomb.cu
+// Loads the FP64 Coulomb kernels' module on the current device (see preload_density_kernels).
+cudaError_t preload_coulomb_kernels();
 // Q splits of the J pass: elems_per_thread = 2 (FP64 B, double2) or 8 (split-BF16 copy).
 int coulomb_nsplit(long tile_elems, long naux, int elems_per_thread);
 // Octet chunks of the mixed w pass; its w buffer holds (1 + chunks) * naux doubles.

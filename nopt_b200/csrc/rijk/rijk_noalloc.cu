@@ -20,9 +20,10 @@
 // Host code cannot pass the array's name to a kernel: on the host it is only a stand-in, not a
 // device address.  rijk_create looks the address up with cudaGetSymbolAddress (with the context's
 // device current) and keeps it in the context.  With CUDA's lazy module loading that lookup is what
-// loads this file's module and allocates the array on the device, so it happens at set-up, while
-// allocating is still allowed, and never inside rijk_coulomb_noalloc.  A context created after a
-// device reset looks the address up again.
+// loads this file's module and allocates the array on the device; the modules of the kernels the call
+// launches (density packing, the Coulomb passes, the unpacking) would likewise load, and allocate, on
+// their first launch, so rijk_create loads them too.  Both happen at set-up, while allocating is still
+// allowed, and never inside rijk_coulomb_noalloc.  A context created after a device reset repeats them.
 #include <cuda_runtime.h>
 
 #include "gemm_f64.cuh"
@@ -39,6 +40,8 @@ namespace rijk {
 int noalloc_resolve(rijk_ctx* ctx) {
   void* p = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&p, g_rijk_noalloc_scratch);
+  if (e == cudaSuccess) e = preload_density_kernels();
+  if (e == cudaSuccess) e = preload_coulomb_kernels();
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? RIJK_ERR_ALLOC : RIJK_ERR_CUDA;
