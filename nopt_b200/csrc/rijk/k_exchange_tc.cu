@@ -870,6 +870,28 @@ static SyrkPlan syrk_plan(long kdim, long tiles, long slots) {
   return {kper, static_cast<int>((kdim + kper - 1) / kper)};
 }
 
+// Split-K plan of the single-CTA SYRK (one CTA per SM at a time): the fewest waves that are at least
+// 90 % full, each CTA at most kMaxChunks 64-wide chunks (its fp32 register sum over the TMEM segments
+// stays as short as the CTA-pair kernel's).  Few, long CTAs pay the pipeline fill and the epilogue once
+// per wave instead of once per short range.
+constexpr long kMaxChunks = 1024;
+static SyrkPlan syrk_plan_waves(long kdim, long tiles, long slots) {
+  const long nchunks = (kdim + 63) / 64;
+  const long smin = std::max<long>(1, (nchunks + kMaxChunks - 1) / kMaxChunks);
+  const long smax = std::max<long>(smin, nchunks / 2);
+  long sp = smin;
+  for (long w = 1; w <= 64; ++w) {
+    const long cand = std::min(smax, (w * slots) / tiles);
+    if (cand < smin) continue;
+    if (static_cast<double>(tiles * cand) >= 0.9 * static_cast<double>(w * slots)) {
+      sp = cand;
+      break;
+    }
+  }
+  const long kper = std::max<long>(2, (nchunks + sp - 1) / sp) * 64;
+  return {kper, static_cast<int>((kdim + kper - 1) / kper)};
+}
+
 // K = sum over orbital batches of X_b^T X_b.  The half-transform holds all orbitals of one batch in
 // the MMA's N dimension (at most 192), so n_c beyond that runs as several batches of equal size; each
 // batch's split-K partials go to their own slots and one reduction sums them all.
@@ -891,7 +913,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
   for (long b0 = 0; b0 < nocc; b0 += per_batch) {
     const long noccp_b = round_up(std::min(per_batch, nocc - b0), 16);
     noccp_max = std::max(noccp_max, noccp_b);
-    const SyrkPlan pl = pair_syrk ? syrk_plan(naux * noccp_b, tiles256, sms / 2) : syrk_plan(naux * noccp_b, ntile128, sms);
+    const SyrkPlan pl = pair_syrk ? syrk_plan(naux * noccp_b, tiles256, sms / 2) : syrk_plan_waves(naux * noccp_b, ntile128, sms);
     nsplit_total += pl.nsplit;
   }
   cudaStream_t s = ctx->stream;
@@ -966,7 +988,7 @@ int mixed_exchange(rijk_ctx* ctx, const double* dMO, long nocc, double* dK) {
       if (rc) return rc;
       slot += pl.nsplit;
     } else {
-      const SyrkPlan pl = syrk_plan(kdim, ntile128, sms);
+      const SyrkPlan pl = syrk_plan_waves(kdim, ntile128, sms);
       SyrkParams sp{};
       sp.kdim = kdim;
       sp.kper = pl.kper;
