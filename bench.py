@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--cpu-slices", type=int, default=12,
                     help="aux slices of the CPU arm when the full-square RI_AA does not fit host memory")
+    ap.add_argument("--metric", default="invsqrt", choices=["invsqrt", "cholesky"],
+                    help="metric factor of the fitted tensor: V^-1/2 (the reference's S05_calc) or L^-1")
     ap.add_argument("--setup", default="gpu", choices=["gpu", "host"],
                     help="gpu: integrals on the device (rijk_set_basis); host: host integrals + rijk_set_3c")
     ap.add_argument("--shard", default="replicas", choices=["replicas", "q"],
@@ -547,10 +549,11 @@ def main():
         q = aux_slices(naux, world)[rank]
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
+    form = rijk.METRIC_CHOLESKY if args.metric == "cholesky" else rijk.METRIC_INVSQRT
     if args.setup == "gpu":  # integrals, metric factor and B all on the device (rijk_set_basis)
-        fb.set_basis(si.orb, si.aux, rijk.METRIC_INVSQRT, *q)
+        fb.set_basis(si.orb, si.aux, form, *q)
     else:  # host integrals up, metric factor and B on the device
-        fb.set_metric(si.V, rijk.METRIC_INVSQRT)
+        fb.set_metric(si.V, form)
         if sharded:
             fb.set_aux_range(*q)
         fb.set_3c(si.I3, n)
@@ -886,6 +889,7 @@ def main():
                "roofline": roof, "coulomb_roofline": coul, "stage_ms": stage_ms,
                "mixed": mixed, "fp64_tc": fp64tc, "scf": scf, "cpu_baseline": cpu, "clocks": clk.summary(),
                "setup": {"path": "rijk_set_basis (GPU integrals)" if args.setup == "gpu" else "host integrals + rijk_set_3c",
+                         "metric": "V^-1/2" if args.metric == "invsqrt" else "L^-1 (Cholesky)",
                          "wall_s": t_setup,
                          "gpu_integrals_ms": st0["ms_setup_ints"] if args.setup == "gpu" else None,
                          "metric_ms": st0["ms_setup_metric"], "b_ms": st0["ms_setup_3c"],

@@ -9,6 +9,8 @@
 // nauxp x nauxp and the raw integrals carry row pitch nauxp, so chunks never straddle.
 // The raw integrals arrive in row-blocks of whole tile rows (I in [I0, I1)); pair rows are
 // gathered per column (NOPT full-square layout or packed mu >= nu layout).
+#include <algorithm>
+
 #include "gemm_f64.cuh"
 #include "rijk_internal.h"
 
@@ -19,7 +21,7 @@ constexpr int K1_THREADS = 128;
 __global__ void __launch_bounds__(K1_THREADS)
     k_metric_contract(const double* __restrict__ M, long nauxp, long mrows, const double* __restrict__ I3, int layout,
                       long n, long naux, long I0, long t0, long rows_in_chunk_base, double* __restrict__ B,
-                      long tile_elems) {
+                      long tile_elems, long tri) {
   extern __shared__ __align__(16) double smem_k1[];
   double* sA[2] = {smem_k1, smem_k1 + 64 * LDK};
   double* sB[2] = {smem_k1 + 2 * 64 * LDK, smem_k1 + 3 * 64 * LDK};
@@ -67,7 +69,9 @@ __global__ void __launch_bounds__(K1_THREADS)
 
   double acc[4][4][2];
   zero_acc(acc);
-  const long nk = nauxp / KC;
+  // tri >= 0: M is lower triangular (the Cholesky factor's inverse), its rows starting at global row
+  // tri, so rows q0 .. q0 + 63 hold zeros past column tri + q0 + 63 and the chunks beyond add nothing
+  const long nk = tri < 0 ? nauxp / KC : std::min(nauxp / KC, (tri + q0 + 64 + KC - 1) / KC);
   load(0, 0);
   cp_async_commit();
   for (long kc = 0; kc < nk; ++kc) {
@@ -100,7 +104,7 @@ __global__ void __launch_bounds__(K1_THREADS)
 // I3 holds the tile rows I in [I0, I1): full layout rows (mu - I0*64)*n + nu, packed layout
 // pair rows starting at pair_base = (I0*64)(I0*64+1)/2.
 void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const double* I3, int layout, long n,
-                                  long naux, long nt, long I0, long I1, double* B, cudaStream_t s) {
+                                  long naux, long nt, long I0, long I1, double* B, cudaStream_t s, long tri) {
   long t0 = tri_index(I0, 0);
   long t1 = tri_index(I1, 0);
   long ntile = nt * (nt + 1) / 2;
@@ -110,7 +114,7 @@ void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const
   const size_t smem = 4 * 64 * LDK * sizeof(double);
   ensure_smem_limit(reinterpret_cast<const void*>(k_metric_contract), smem);
   k_metric_contract<<<grid, K1_THREADS, smem, s>>>(M, nauxp, mrows, I3, layout, n, naux, I0, t0, pair_base, B,
-                                                   ntile * TILE2);
+                                                   ntile * TILE2, tri);
 }
 
 }  // namespace rijk

@@ -563,7 +563,8 @@ int set_3c_impl(rijk_ctx* ctx, long n, long naux, int layout, const ChunkFill& f
     cudaEventRecord(ctx->ev0, s);
     launch_metric_contract_chunk(static_cast<const double*>(ctx->M.p) + q0 * nauxp, nauxp, nauxp - q0,
                                  static_cast<const double*>(raw.p), layout, n, nq, nt, I0, I1,
-                                 static_cast<double*>(ctx->B.p), s);
+                                 static_cast<double*>(ctx->B.p), s,
+                                 ctx->metric_form == RIJK_METRIC_CHOLESKY ? q0 : -1);
     cudaEventRecord(ctx->ev1, s);
     rc = cuda_check(ctx, cudaStreamSynchronize(s), "metric contraction");
     if (rc) { release(raw); return rc; }

@@ -181,9 +181,11 @@ void launch_scan_nonfinite(const double* x, long count, int* err, cudaStream_t s
 
 // ---- k_metric.cu
 // B[Q][tile-packed e] = sum_P M[Q][P] * I3(pair(e), P) for the raw rows of tile rows [I0, I1).
-// M may start at a row offset q0 (mrows = rows left after it); B receives naux rows.
+// M may start at a row offset q0 (mrows = rows left after it); B receives naux rows.  tri >= 0 declares
+// M lower triangular with its first row at global row tri (the Cholesky form): the contraction then
+// stops at each row block's last nonzero column, half the products, the same result.
 void launch_metric_contract_chunk(const double* M, long nauxp, long mrows, const double* I3, int layout, long n,
-                                  long naux, long nt, long I0, long I1, double* B, cudaStream_t s);
+                                  long naux, long nt, long I0, long I1, double* B, cudaStream_t s, long tri = -1);
 
 // ---- k_coulomb.cu
 // Loads the FP64 Coulomb kernels' module on the current device (see preload_density_kernels).
