@@ -38,7 +38,7 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 NCU_TRAFFIC = {("h2o16_dz", "xform_f64"): 1.277529e9 + 0.437618e9,
                ("h2o16_dz", "syrk_f64"): 0.457111e9 + 0.092111e9,
                ("h2o16_dz", "xform_tc"): 0.639337e9 + 0.202236e9,
-               ("h2o16_dz", "syrk_tc"): 0.228261e9 + 0.030061e9,
+               ("h2o16_dz", "syrk_tc"): 0.229277e9 + 0.004902e9,
                ("h2o16_dz", "syrk_i8"): 0.970246e9 + 0.088795e9,
                ("h2o16_dz", "coulomb_w_mixed"): 0.639341e9 + 0.004234e9,
                ("h2o16_dz", "coulomb_j_mixed"): 0.638610e9 + 0.010762e9,
