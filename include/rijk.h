@@ -28,6 +28,11 @@
  * One context drives one GPU.  A context is not thread-safe.  Every function returns
  * RIJK_OK (0) or a negative RIJK_ERR_* code; rijk_last_error() gives the message.  Nothing
  * in the library calls exit() or aborts.
+ *
+ * With the environment variable RIJK_LOG set to a file name, every Fock build (rijk_fock; a
+ * rijk_fock_device build at its rijk_sync) and every rijk_scf appends one JSON line to that file:
+ * sizes, precision, device times, algorithmic FLOPs and bytes and their rates.  The main calls
+ * are NVTX ranges of their own names for timeline tools.
  */
 #ifndef RIJK_H
 #define RIJK_H
@@ -181,6 +186,13 @@ int rijk_sync(rijk_ctx* ctx);
  * frees the TMEM and returns.  Asynchronous; the next rijk_sync returns RIJK_ERR_TIMEOUT, and the
  * context stays usable. */
 int rijk_selftest_wait_timeout(rijk_ctx* ctx, long long cycles);
+
+/* Self-test of the allocation failure paths (no reference counterpart): after `after` more device
+ * allocations of this context succeed, the next one fails with RIJK_ERR_ALLOC, as an exhausted
+ * cudaMalloc would, and every later one too, until the hook is turned off with after < 0.  Only
+ * allocations the library would really make count (a buffer already large enough is reused).  A
+ * failed call leaves the context usable once allocations succeed again. */
+int rijk_selftest_alloc_failure(rijk_ctx* ctx, long after);
 
 /* Size of the fixed device scratch used by rijk_coulomb_noalloc (per GPU, held until exit). */
 #define RIJK_NOALLOC_SCRATCH_BYTES (32L * 1024 * 1024)

@@ -193,6 +193,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   int rc = check_fock_args(ctx, nocc, RIJK_PREC_FP64);
   if (rc) return rc;
   if (nocc < 1) return set_err(ctx, RIJK_ERR_ARG, "rijk_grad: n_c must be at least 1");
+  NvtxRange range("rijk_grad");
   if (ctx->nq != ctx->naux)
     return set_err(ctx, RIJK_ERR_STATE, "rijk_grad needs all aux functions in one context (no aux range)");
   cudaSetDevice(ctx->device);

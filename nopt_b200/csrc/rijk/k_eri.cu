@@ -791,6 +791,7 @@ RIJK_API int rijk_eri3c(rijk_ctx* ctx, const rijk_basis_t* orb, const rijk_basis
 
 RIJK_API int rijk_set_basis(rijk_ctx* ctx, const rijk_basis_t* orb, const rijk_basis_t* aux, int metric_form, long q0,
                             long q1) {
+  rijk::NvtxRange range("rijk_set_basis");
   if (!ctx) return RIJK_ERR_ARG;
   if (!orb) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_basis: null orbital basis");
   cudaSetDevice(ctx->device);

@@ -20,6 +20,7 @@
 // the memory layout of the reference's MO_VEC (row i = orbital i), so its first n_c columns
 // are passed to the Fock build as MO.
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -428,6 +429,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
                       const rijk_scf_opts_t* opts, double* MO, rijk_scf_result_t* result) {
   if (!ctx) return RIJK_ERR_ARG;
   if (!H || !S || !result) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: null pointer");
+  NvtxRange range("rijk_scf");
   rijk_scf_opts_t o{};
   if (opts) o = *opts;
   if (o.max_iter <= 0) o.max_iter = 100;
@@ -1086,6 +1088,15 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   result->ms_final_phase = std::chrono::duration<double, std::milli>(t_end - t_loop1).count();
   result->purified = purified;
   cleanup();
+  {
+    char buf[384];
+    std::snprintf(buf, sizeof(buf),
+                  "{\"call\": \"rijk_scf\", \"device\": %d, \"n\": %ld, \"naux\": %ld, \"n_c\": %ld, "
+                  "\"energy\": %.12f, \"iterations\": %d, \"iterations_mixed\": %d, \"converged\": %d, "
+                  "\"ms_total\": %.6g, \"ms_fock\": %.6g}",
+                  ctx->device, n, ctx->naux, nocc, E, nbuild, nmix, converged ? 1 : 0, result->ms_total, ms_fock);
+    log_line(buf);
+  }
   if (!converged) return set_err(ctx, RIJK_ERR_CONVERGE, "rijk_scf: not converged in %d iterations", o.max_iter);
   return RIJK_OK;
 }

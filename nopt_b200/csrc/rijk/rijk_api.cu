@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -44,6 +45,10 @@ int cuda_check(rijk_ctx* ctx, cudaError_t e, const char* what) {
 
 int ensure(rijk_ctx* ctx, DeviceBuf& b, size_t bytes, const char* what) {
   if (b.bytes >= bytes && b.p) return RIJK_OK;
+  if (bytes > 0 && ctx->fail_alloc_after >= 0) {  // rijk_selftest_alloc_failure
+    if (ctx->fail_alloc_after == 0) return set_err(ctx, RIJK_ERR_ALLOC, "%s: out of device memory (injected)", what);
+    --ctx->fail_alloc_after;
+  }
   if (b.p) {  // the old buffer may still be read by work queued on the context's streams
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
@@ -115,6 +120,40 @@ __global__ void k_fock_matrix(const double* __restrict__ H, const double* __rest
 static unsigned grid1d(long total) {
   long b = (total + 255) / 256;
   return static_cast<unsigned>(std::min<long>(std::max<long>(b, 1), 148L * 16));
+}
+
+namespace {
+std::mutex g_log_mu;
+FILE* g_log = nullptr;
+bool g_log_checked = false;
+}  // namespace
+
+void log_line(const std::string& json) {
+  std::lock_guard<std::mutex> lock(g_log_mu);
+  if (!g_log_checked) {
+    g_log_checked = true;
+    const char* path = std::getenv("RIJK_LOG");
+    if (path && *path) g_log = std::fopen(path, "a");
+  }
+  if (!g_log) return;
+  std::fputs(json.c_str(), g_log);
+  std::fputc('\n', g_log);
+  std::fflush(g_log);
+}
+
+void log_build(rijk_ctx* ctx, const char* call, long nocc, int precision) {
+  const rijk_stats_t& st = ctx->stats;
+  const char* prec = precision == RIJK_PREC_MIXED ? "mixed" : precision == RIJK_PREC_FP64_TC ? "fp64_tc" : "fp64";
+  const double ms = st.ms_last_fock;
+  char buf[640];
+  std::snprintf(buf, sizeof(buf),
+                "{\"call\": \"%s\", \"device\": %d, \"n\": %ld, \"naux\": %ld, \"q0\": %ld, \"n_c\": %ld, "
+                "\"precision\": \"%s\", \"ms\": %.6g, \"ms_coulomb\": %.6g, \"ms_exchange\": %.6g, "
+                "\"flops\": %.6g, \"bytes\": %.6g, \"tflops\": %.6g, \"gbs\": %.6g, \"kernels\": %d}",
+                call, ctx->device, ctx->n, ctx->nq, ctx->q0, nocc, prec, ms, st.ms_coulomb, st.ms_exchange,
+                st.flops_last_fock, st.bytes_last_fock, ms > 0 ? st.flops_last_fock / (ms * 1e9) : 0.0,
+                ms > 0 ? st.bytes_last_fock / (ms * 1e6) : 0.0, st.kernels_last_fock);
+  log_line(buf);
 }
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
@@ -372,6 +411,7 @@ RIJK_API int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1) {
 
 RIJK_API int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int form) {
   if (!ctx) return RIJK_ERR_ARG;
+  NvtxRange range("rijk_set_metric");
   return set_metric_impl(ctx, PQ, cudaMemcpyHostToDevice, naux, form);
 }
 
@@ -488,6 +528,7 @@ int set_metric_impl(rijk_ctx* ctx, const double* PQ, cudaMemcpyKind kind, long n
 RIJK_API int rijk_set_3c(rijk_ctx* ctx, const double* I3, long n, long naux, int layout) {
   if (!ctx) return RIJK_ERR_ARG;
   if (!I3 || n <= 0 || naux <= 0) return set_err(ctx, RIJK_ERR_ARG, "rijk_set_3c: null integrals or bad sizes");
+  NvtxRange range("rijk_set_3c");
   cudaStream_t s = ctx->stream;
   return set_3c_impl(ctx, n, naux, layout, [&](long, long, long first, long count, double* raw, long ld) {
     if (count <= 0) return static_cast<int>(RIJK_OK);
@@ -610,6 +651,10 @@ RIJK_API int rijk_sync(rijk_ctx* ctx) {
   ctx->stats.ms_coulomb = elapsed(ctx->ev0, ctx->ev1);
   ctx->stats.ms_exchange = elapsed(ctx->ev1, ctx->ev2);
   ctx->stats.ms_last_fock = elapsed(ctx->ev0, ctx->ev2);
+  if (ctx->log_pending) {
+    ctx->log_pending = false;
+    log_build(ctx, "rijk_fock_device", ctx->log_nocc, ctx->log_precision);
+  }
   return RIJK_OK;
 }
 
@@ -630,8 +675,15 @@ RIJK_API int rijk_fock_device(rijk_ctx* ctx, const double* dD, const double* dMO
   if (!dD || !dJ || !dK || (nocc > 0 && !dMO)) return set_err(ctx, RIJK_ERR_ARG, "rijk_fock_device: null pointer");
   int rc = check_fock_args(ctx, nocc, precision);
   if (rc) return rc;
+  NvtxRange range("rijk_fock_device");
   cudaSetDevice(ctx->device);
-  return fock_device_impl(ctx, dD, dMO, nocc, dJ, dK, precision);
+  rc = fock_device_impl(ctx, dD, dMO, nocc, dJ, dK, precision);
+  if (!rc) {
+    ctx->log_pending = true;
+    ctx->log_nocc = nocc;
+    ctx->log_precision = precision;
+  }
+  return rc;
 }
 
 RIJK_API int rijk_fock(rijk_ctx* ctx, const double* D, const double* MO, long nocc, double* J, double* K,
@@ -640,6 +692,7 @@ RIJK_API int rijk_fock(rijk_ctx* ctx, const double* D, const double* MO, long no
   if (!D || !J || !K || (nocc > 0 && !MO)) return set_err(ctx, RIJK_ERR_ARG, "rijk_fock: null pointer");
   int rc = check_fock_args(ctx, nocc, precision);
   if (rc) return rc;
+  NvtxRange range("rijk_fock");
   cudaSetDevice(ctx->device);
   const long n = ctx->n;
   const size_t nn = static_cast<size_t>(n) * n * sizeof(double);
@@ -676,6 +729,8 @@ RIJK_API int rijk_fock(rijk_ctx* ctx, const double* D, const double* MO, long no
   ctx->stats.ms_coulomb = elapsed(ctx->ev0, ctx->ev1);
   ctx->stats.ms_exchange = elapsed(ctx->ev1, ctx->ev2);
   ctx->stats.ms_last_fock = elapsed(ctx->ev0, ctx->ev2);
+  ctx->log_pending = false;
+  log_build(ctx, "rijk_fock", nocc, precision);
   return RIJK_OK;
 }
 

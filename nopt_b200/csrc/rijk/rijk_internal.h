@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cstdint>
 #include <functional>
 #include <string>
@@ -39,6 +41,14 @@ constexpr int DEVERR_BOUNDS = 4;
 struct DeviceBuf {
   void* p = nullptr;
   size_t bytes = 0;
+};
+
+// An NVTX range around one C-ABI call, for timeline tools (Nsight Systems); free when no tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 }  // namespace rijk
@@ -80,6 +90,11 @@ struct rijk_ctx {
   rijk::DeviceBuf Xe;       // their row exponents, parts x npad2
   rijk::DeviceBuf scf[32];  // rijk_scf's work buffers, kept between calls
   double* noalloc_scratch = nullptr;  // device address of rijk_coulomb_noalloc's fixed scratch on `device`
+  long fail_alloc_after = -1;  // rijk_selftest_alloc_failure: allocations left before one is refused (-1: off)
+  // a device build queued by rijk_fock_device, written to the metrics log by the next rijk_sync
+  bool log_pending = false;
+  long log_nocc = 0;
+  int log_precision = 0;
   // streaming three-centre input (rijk_begin_3c / rijk_add_3c_block) in progress
   struct {
     bool active = false;
@@ -119,6 +134,11 @@ int check_device_error(rijk_ctx* ctx);
 // process: a process that drives several GPUs sets it on each.
 cudaError_t ensure_smem_limit(const void* fn, size_t bytes);
 int check_fock_args(rijk_ctx* ctx, long nocc, int precision);
+// One JSON line per Fock build (and per rijk_scf) appended to the file named by the environment
+// variable RIJK_LOG, when it is set: the call, sizes, precision, device times, algorithmic FLOPs and
+// bytes and the rates they give.  Nothing is written when RIJK_LOG is unset.
+void log_build(rijk_ctx* ctx, const char* call, long nocc, int precision);
+void log_line(const std::string& json);
 // One Fock build on device pointers (J into dJ, K into dK), asynchronous on ctx->stream.  With
 // mo_ready the exchange waits for that event (dMO is written on another stream); with j_done the
 // event is recorded once J is complete, before the exchange kernels.

@@ -7,6 +7,10 @@
 // fault: one warp allocates TMEM as the exchange kernels do, waits on an mbarrier that nothing ever
 // arrives on, with a short cycle limit, gives up, raises the error bit, frees the TMEM and returns.
 // The context stays usable afterwards.
+//
+// rijk_selftest_alloc_failure makes the context's own device allocations run out on purpose, on the host:
+// the chosen allocation returns RIJK_ERR_ALLOC as a cudaMalloc out of memory would, so that every
+// call's allocation failure path can be exercised without exhausting a GPU.
 #include <cuda_runtime.h>
 
 #include "rijk_internal.h"
@@ -59,4 +63,10 @@ RIJK_API int rijk_selftest_wait_timeout(rijk_ctx* ctx, long long cycles) {
   if (e != cudaSuccess) return cuda_check(ctx, e, "rijk_selftest_wait_timeout: cudaSetDevice");
   k_wait_probe<<<1, 32, 0, ctx->stream>>>(static_cast<int*>(ctx->err.p), cycles);
   return cuda_check(ctx, cudaGetLastError(), "rijk_selftest_wait_timeout launch");
+}
+
+RIJK_API int rijk_selftest_alloc_failure(rijk_ctx* ctx, long after) {
+  if (!ctx) return RIJK_ERR_ARG;
+  ctx->fail_alloc_after = after < 0 ? -1 : after;
+  return RIJK_OK;
 }

@@ -88,6 +88,7 @@ RIJK_API int rijk_add_3c_block(rijk_ctx* ctx, long mu0, long mu1, const double* 
   const long n = ctx->s3.n, naux = ctx->s3.naux;
   const int layout = ctx->s3.layout;
   if (!block) return set_err(ctx, RIJK_ERR_ARG, "rijk_add_3c_block: null block");
+  NvtxRange range("rijk_add_3c_block");
   if (mu0 != ctx->s3.next_mu || mu1 <= mu0 || mu1 > n)
     return set_err(ctx, RIJK_ERR_ARG, "rijk_add_3c_block: rows [%ld, %ld) do not continue at row %ld (n_ao = %ld)", mu0,
                    mu1, ctx->s3.next_mu, n);

@@ -126,6 +126,7 @@ def lib():
         L.rijk_fock_device.argtypes = [_vp, _vp, _vp, ctypes.c_long, _vp, _vp, ctypes.c_int]
         L.rijk_sync.argtypes = [_vp]
         L.rijk_selftest_wait_timeout.argtypes = [_vp, ctypes.c_longlong]
+        L.rijk_selftest_alloc_failure.argtypes = [_vp, ctypes.c_long]
         L.rijk_coulomb_noalloc.argtypes = [_vp, _vp, _vp]
         L.rijk_grad.argtypes = [_vp, _dp, ctypes.c_long, _dp, ctypes.c_double, _dp, _dp, _dp, _dp]
         L.rijk_mo_ints.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_long, ctypes.c_long, ctypes.c_long]
@@ -376,6 +377,11 @@ class FockBuilder:
 
     def sync(self):
         self._check(lib().rijk_sync(self._h))
+
+    def selftest_alloc_failure(self, after):
+        """After `after` more device allocations of this context, refuse the next ones with ERR_ALLOC
+        (after < 0: off)."""
+        self._check(lib().rijk_selftest_alloc_failure(self._h, int(after)))
 
     def selftest_wait_timeout(self, cycles):
         """Launch the bounded-wait self-test (a wait that runs out after `cycles` SM clocks); the
