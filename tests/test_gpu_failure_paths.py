@@ -34,7 +34,7 @@ def hexamer():
     return si, DM, MO, Jr, Kr
 
 
-def _run_with_failures(call, setup=None, max_k=40):
+def _run_with_failures(call, setup=None, max_k=96):
     """call(fb) under an allocation refused after k successes, k = 0, 1, ...: each attempt on a fresh
     context either fails with ERR_ALLOC or succeeds; after a failure the same call on the same context,
     allocations allowed again, must succeed.  Returns the number of allocation points met."""
