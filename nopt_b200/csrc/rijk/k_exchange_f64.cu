@@ -131,12 +131,13 @@ static void launch_xform_batches(int nf, const double* B, const double* MOp, lon
 // The orbitals go in batches of at most 96 (NF <= 6 keeps the accumulators in registers).  The
 // full-size batches run in one launch (each tile column's batches back to back, B^Q read once from
 // HBM); a smaller last batch gets a launch of its own.
-void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s) {
+int launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s) {
   const long nbatch = (noccp + 95) / 96;
   const long per = round_up((noccp + nbatch - 1) / nbatch, 16);
   const long nfull = noccp / per, rest = noccp - nfull * per;
   if (nfull > 0) launch_xform_batches(static_cast<int>(per / 16), B, MOp, naux, nt, noccp, 0, static_cast<int>(nfull), XT, s);
   if (rest > 0) launch_xform_batches(static_cast<int>(rest / 16), B, MOp, naux, nt, noccp, nfull * per, 1, XT, s);
+  return (nfull > 0 ? 1 : 0) + (rest > 0 ? 1 : 0);
 }
 
 constexpr int S_THREADS = 128;

@@ -249,8 +249,8 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
       return rc;
     launch_pack_mo(dMO, nocc, n, noccp, npad, static_cast<double*>(ctx->MOp.p), s);
     prof_mark(ctx, "pack_mo");
-    launch_xform_f64(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->MOp.p), naux, nt, noccp,
-                     static_cast<double*>(ctx->XT.p), s);
+    launches += launch_xform_f64(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->MOp.p), naux,
+                                 nt, noccp, static_cast<double*>(ctx->XT.p), s);
     prof_mark(ctx, "xform_f64");
     if (tc) {  // int8 digit planes of X^T, then K on tcgen05 (exact s32 products)
       rc = syrk_i8(ctx, static_cast<const double*>(ctx->XT.p), npad, nt, kdim, nsK, kper_tc,
@@ -265,7 +265,7 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
     }
     launch_unpack_sym(static_cast<double*>(ctx->Kpart.p), nsK, ntile, n, dK, s);
     prof_mark(ctx, "unpack_k");
-    launches += 4;
+    launches += 3 + (nsK > 1 ? 1 : 0);  // pack_mo, syrk, unpack (+ split sum); the half-transform counted above
   }
   cudaEventRecord(ctx->ev2, s);
   rc = cuda_check(ctx, cudaGetLastError(), "fock launch");

@@ -225,7 +225,8 @@ void launch_coulomb_j_mixed(const __nv_bfloat16* Bmix, const double* w, long nau
                             int nsplit, double* Jpart, cudaStream_t s);
 
 // ---- k_exchange_f64.cu
-void launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s);
+// Returns the number of kernel launches it made (one, or two when a smaller last orbital batch remains).
+int launch_xform_f64(const double* B, const double* MOp, long naux, long nt, long noccp, double* XT, cudaStream_t s);
 int syrk_nsplit(long nt, long kdim);
 void launch_syrk_f64(const double* XT, long npad, long nt, long kdim, int nsplit, double* Kpart, cudaStream_t s);
 
