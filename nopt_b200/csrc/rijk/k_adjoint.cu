@@ -16,8 +16,8 @@
 //
 // Device work, FP64 throughout, every contraction on hand-written DMMA kernels: one FP64 Fock build
 // (which leaves w and the half-transformed XT in the context), then, over chunks of aux functions,
-// the small batched products Y^Q = X^Q C^T and T^Q = Y^Q C (k_gemm_f64), k_gamma_f64 forming the
-// packed Gamma tiles Gamma^Q_tile = 4 w_Q D_tile - 2 T^Q_rows Ct_cols^T, and two contractions of
+// the products Y^Q = X^Q C^T and T^Q = Y^Q C for every Q of the chunk at once (k_gemm_f64), k_gamma_f64
+// forming the packed Gamma tiles Gamma^Q_tile = 4 w_Q D_tile - 2 T^Q_rows Ct_cols^T, and two contractions of
 // the chunk of Gamma: with M, written straight into the packed pair layout of dE/d(P|mu nu)
 // (accumulated over chunks), and with B, the chunk's rows of G (diagonal tiles weighted 1/2).  When
 // HBM cannot hold Gamma for every aux function at once, each chunk's X^Q is recomputed in tiles
@@ -36,30 +36,33 @@ namespace {
 
 constexpr int G_THREADS = 128;
 
-// Gamma[Q][t][r][c] = 4 w_Q D[mu][nu] - 2 sum_i T[Q][mu][i] Ct[nu][i], tile t = (I, J), I >= J.
-// T: [naux][npad][noccp] (row mu, i contiguous); Ct: [npad][noccp]; D: n x n.
+// Gamma[Q][t][r][c] = 4 w_Q D[mu][nu] - 2 sum_i T^Q[mu][i] Ct[nu][i], tile t = (I, J), I >= J.
+// Tt: [(Q, i)][npad] = T^Q transposed (row (Q, i), mu contiguous); Ct: [npad][noccp]; D: n x n.
+constexpr int G_ASTAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
 __global__ void __launch_bounds__(G_THREADS)
-    k_gamma_f64(const double* __restrict__ T, const double* __restrict__ Ct, const double* __restrict__ D,
+    k_gamma_f64(const double* __restrict__ Tt, const double* __restrict__ Ct, const double* __restrict__ D,
                 const double* __restrict__ w, long n, long npad, long noccp, long tile_elems,
                 double* __restrict__ Gamma) {
   extern __shared__ __align__(16) double smem_g[];
-  double* sA[2] = {smem_g, smem_g + 64 * LDK};
-  double* sB[2] = {smem_g + 2 * 64 * LDK, smem_g + 3 * 64 * LDK};
+  double* sA[2] = {smem_g, smem_g + G_ASTAGE};
+  double* sB[2] = {smem_g + 2 * G_ASTAGE, smem_g + 2 * G_ASTAGE + 64 * LDK};
   const long t = blockIdx.x, Q = blockIdx.y;
   long I, J;
   tri_decode(t, I, J);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
-  const double* Ar = T + (Q * npad + I * TILE) * noccp;
+  const double* Ar = Tt + Q * noccp * npad + I * TILE;  // A(mu, i) = Ar[i * npad + mu]: staged [i][mu]
   const double* Br = Ct + J * TILE * noccp;
   auto load = [&](int stage, long k0) {
 #pragma unroll
     for (int it = 0; it < 8; ++it) {
       int idx = tid + it * G_THREADS;
-      int row = idx >> 4, seg = idx & 15;
+      int ka = idx >> 5, pa = idx & 31;  // A: k row (i) 0..31, mu pair 0..31
+      bool oka = k0 + ka < noccp;
+      cp_async16(&sA[stage][ka * LDM + pa * 2], oka ? Ar + (k0 + ka) * npad + pa * 2 : Tt, oka);
+      int row = idx >> 4, seg = idx & 15;  // B: row nu 0..63, i pair 0..15
       long k = k0 + seg * 2;
       bool ok = k < noccp;
-      cp_async16(&sA[stage][row * LDK + seg * 2], ok ? Ar + row * noccp + k : T, ok);
       cp_async16(&sB[stage][row * LDK + seg * 2], ok ? Br + row * noccp + k : Ct, ok);
     }
   };
@@ -77,7 +80,7 @@ __global__ void __launch_bounds__(G_THREADS)
       cp_async_wait<0>();
     }
     __syncthreads();
-    warp_mma_chunk<4, 4, true>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * 32, lane);
+    warp_mma_chunk<4, 4, false>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * 32, lane);
     __syncthreads();
   }
   const int g = lane >> 2, tq = lane & 3;
@@ -304,7 +307,7 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
   double* pGam = static_cast<double*>(Gam.p);
   double* pY = static_cast<double*>(Y.p);
   double* pT = static_cast<double*>(Tb.p);
-  const size_t gsmem = 4 * 64 * LDK * sizeof(double);
+  const size_t gsmem = (2 * G_ASTAGE + 2 * 64 * LDK) * sizeof(double);
   ensure_smem_limit(reinterpret_cast<const void*>(k_gamma_f64), gsmem);
   for (long q0 = 0; q0 < naux; q0 += qc) {
     const long nq = std::min(qc, naux - q0);
@@ -319,21 +322,22 @@ RIJK_API int rijk_grad(rijk_ctx* ctx, const double* MO, long nocc, const double*
       X = static_cast<const double*>(ctx->XT.p) + q0 * noccp;
       ldx = kdim;
     }
-    {  // Y^Q[i][j] = sum_nu X^Q_{i nu} C_{j nu}   (= C B^Q C^T)
+    {  // Y^Q[i][j] = sum_nu X^Q_{i nu} C_{j nu} (= C B^Q C^T), every Q of the chunk in one product:
+       // rows (Q, i) of X^T's columns are contiguous, so Y[(Q, i)][j] is one GEMM over nu
       GemmF64Args g;
-      g.M = noccp, g.N = noccp, g.K = npad;
-      g.A = X, g.lda = ldx, g.sA = noccp, g.a_kmajor = false;
-      g.B = MOp, g.ldb = npad, g.sB = 0, g.b_kmajor = true;
-      g.C = pY, g.ldc = noccp, g.sC = noccp * noccp;
-      gemm_f64(g, nq, s);
+      g.M = nq * noccp, g.N = noccp, g.K = npad;
+      g.A = X, g.lda = ldx, g.a_kmajor = false;
+      g.B = MOp, g.ldb = npad, g.b_kmajor = true;
+      g.C = pY, g.ldc = noccp;
+      gemm_f64(g, 1, s);
     }
-    {  // T^Q[mu][i] = sum_j C_{j mu} Y^Q[j][i]
+    {  // T^Q transposed, Tt[(Q, i)][mu] = sum_j Y^Q[i][j] C_{j mu}: again one GEMM for the chunk
       GemmF64Args g;
-      g.M = npad, g.N = noccp, g.K = noccp;
-      g.A = MOp, g.lda = npad, g.sA = 0, g.a_kmajor = false;
-      g.B = pY, g.ldb = noccp, g.sB = noccp * noccp, g.b_kmajor = false;
-      g.C = pT, g.ldc = noccp, g.sC = npad * noccp;
-      gemm_f64(g, nq, s);
+      g.M = nq * noccp, g.N = npad, g.K = noccp;
+      g.A = pY, g.lda = noccp, g.a_kmajor = true;
+      g.B = MOp, g.ldb = npad, g.b_kmajor = false;
+      g.C = pT, g.ldc = npad;
+      gemm_f64(g, 1, s);
     }
     tm.mark(2);
     dim3 grid(static_cast<unsigned>(ntile), static_cast<unsigned>(nq));
