@@ -99,7 +99,8 @@ def _random_problem(n, naux, seed):
 
 
 @pytest.mark.parametrize("n,naux,nocc", [(70, 100, 13), (64, 33, 16), (1, 5, 1), (130, 257, 0), (200, 96, 97),
-                                         (200, 96, 161), (180, 40, 130), (300, 64, 282)])
+                                         (200, 96, 161), (180, 40, 130), (150, 70, 113), (260, 50, 160),
+                                         (300, 64, 282)])
 def test_jk_parity_ragged_random(n, naux, nocc):
     V, I3 = _random_problem(n, naux, n + naux)
     rng = np.random.default_rng(7)
