@@ -50,6 +50,7 @@ extern "C" {
 #define RIJK_ERR_TIMEOUT -6  /* a bounded device-side wait ran out                             */
 #define RIJK_ERR_NUMERIC -7  /* NaN or Inf met in an input or a result                        */
 #define RIJK_ERR_CONVERGE -8 /* SCF did not converge within the iteration limit                */
+#define RIJK_ERR_REDUCE -9   /* the caller's J/K reduction (rijk_scf_opts_t.reduce_jk) failed    */
 
 /* Metric forms.  J and K agree in exact arithmetic (L^-T L^-1 = V^-1 = V^-1/2 V^-1/2). */
 #define RIJK_METRIC_INVSQRT 0  /* V^-1/2 by eigendecomposition, eigenvalues <= 0 dropped (S05_calc) */
@@ -111,7 +112,8 @@ int rijk_set_metric(rijk_ctx* ctx, const double* PQ, long naux, int metric_form)
 /* Hold only the aux functions [q0, q1) of the fitted tensor (call after rijk_set_metric,
  * before rijk_set_3c).  J, K and rijk_mo_ints are sums over the aux index, so a Fock build of
  * such a context returns the slice's partial J and K; contexts on several GPUs that cover
- * [0, naux) give the full J and K after one all-reduce (sum).  rijk_scf and rijk_grad need
+ * [0, naux) give the full J and K after one all-reduce (sum).  rijk_scf runs on a slice with a
+ * reduce_jk callback in its options (the sum over the ranks after every build); rijk_grad needs
  * the whole range. */
 int rijk_set_aux_range(rijk_ctx* ctx, long q0, long q1);
 
@@ -261,6 +263,20 @@ typedef struct {
    * receives n_proj (less dropped) orbitals as rows of n_ao coefficients, the rest zero.        */
   const double* ao_projector;
   long n_proj;            /* 1 .. n_ao                                                          */
+  /* Aux-sharded SCF (appended fields; NULL = one context holds every aux function).  Each rank's
+   * context holds one slice of the aux functions (rijk_set_aux_range), so its Fock builds give
+   * partial J and K.  rijk_scf calls reduce_jk(jk, count, stream, reduce_user) after every build,
+   * with jk the device array [J | K] (count = 2 n_ao^2 doubles) written by work on `stream` (the
+   * context's cudaStream_t).  The callback replaces jk in place by its sum over the ranks, either
+   * enqueued on `stream` (an NCCL all-reduce) or complete when it returns (a host reduction after
+   * synchronising the stream), and returns 0; any other value ends rijk_scf with RIJK_ERR_REDUCE.
+   * Every rank calls rijk_scf with the same arguments.  The steps after the reduction use no
+   * floating-point atomics, so equal J and K give equal decisions (DIIS, switch, convergence) on
+   * every rank and the ranks reach the reduction the same number of times.  A context holding an
+   * aux range needs reduce_jk; one holding every aux function calls it too when it is given (a
+   * one-rank group).                                                                               */
+  int (*reduce_jk)(double* jk, long count, void* stream, void* user);
+  void* reduce_user;
 } rijk_scf_opts_t;
 
 #define RIJK_CONV_DIIS 0

@@ -11,6 +11,7 @@
 //       are formed, split over k into nsplit ranges whose partial tiles are summed (and
 //       mirrored) by the unpack kernel.  FLOPs n(n+1) noccp naux, the SYRK count.
 #include <algorithm>
+#include <atomic>
 
 #include "gemm_f64.cuh"
 #include "rijk_internal.h"
@@ -207,7 +208,7 @@ constexpr size_t kSyrkSmem = 4 * 64 * LDK * sizeof(double);
 
 // CTAs of k_syrk_f64 resident per SM (registers and shared memory), from the runtime.
 int syrk_ctas_per_sm() {
-  static int slots[64] = {};
+  static std::atomic<int> slots[64] = {};  // contexts on other host threads may ask at once
   int dev = 0;
   cudaGetDevice(&dev);
   ensure_smem_limit(reinterpret_cast<const void*>(k_syrk_f64), kSyrkSmem);

@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 
@@ -342,14 +343,15 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiledFn encode_fn_i8() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* q = nullptr;
-    cudaDriverEntryPointQueryResult r;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &q, cudaEnableDefault, &r) == cudaSuccess &&
-        r == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(q);
-  }
+  // looked up once (thread-safe static initialisation: contexts may live on several host threads)
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      return reinterpret_cast<EncodeTiledFn>(p);
+    return static_cast<EncodeTiledFn>(nullptr);
+  }();
   return fn;
 }
 
@@ -368,7 +370,7 @@ bool make_map_i8(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows,
 }
 
 int sm_count(int device) {
-  static int cached[64] = {};
+  static std::atomic<int> cached[64] = {};
   if (device < 0 || device >= 64) return 148;
   if (!cached[device]) {
     int v = 0;

@@ -21,6 +21,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "rijk_internal.h"
@@ -764,14 +765,15 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
+  // looked up once (thread-safe static initialisation: contexts may live on several host threads)
+  static const EncodeTiledFn fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
+      return reinterpret_cast<EncodeTiledFn>(p);
+    return static_cast<EncodeTiledFn>(nullptr);
+  }();
   return fn;
 }
 
@@ -790,7 +792,7 @@ bool make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, ui
 }
 
 int num_sms(int device) {
-  static int cached[64] = {};
+  static std::atomic<int> cached[64] = {};
   if (device >= 0 && device < 64 && cached[device]) return cached[device];
   int v = 148;
   cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);

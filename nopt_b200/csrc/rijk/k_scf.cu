@@ -454,8 +454,10 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   if (o.diis_size > 32) return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: diis_size above 32");
   if (o.guess_dm && (!o.guess_rows || o.guess_nrows <= 0 || o.guess_nrows > round_up(ctx->n, 16)))
     return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: guess needs factor rows (1 .. n_ao of them)");
-  if (ctx->nq != ctx->naux)
-    return set_err(ctx, RIJK_ERR_STATE, "rijk_scf needs all aux functions in one context (no aux range)");
+  if (ctx->nq != ctx->naux && !o.reduce_jk)
+    return set_err(ctx, RIJK_ERR_STATE,
+                   "rijk_scf on an aux range [%ld, %ld) needs opts->reduce_jk to sum J and K over the ranks", ctx->q0,
+                   ctx->q0 + ctx->nq);
   if (o.ao_projector && (o.n_proj < 1 || o.n_proj > ctx->n))
     return set_err(ctx, RIJK_ERR_ARG, "rijk_scf: n_proj = %ld outside [1, n_ao = %ld]", o.n_proj, ctx->n);
   cudaSetDevice(ctx->device);
@@ -471,7 +473,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   // call then makes no cudaMalloc / cudaFree, whose frees synchronise the device.
   DeviceBuf* wb = ctx->scf;
   DeviceBuf &dH = wb[0], &dS = wb[1], &dX = wb[2], &dF = wb[3], &dFex = wb[4], &dD = wb[5], &dDn = wb[6],
-            &dC = wb[7], &dJ = wb[8], &dK = wb[9], &dT1 = wb[10], &dT2 = wb[11], &dE = wb[12], &dW = wb[13],
+            &dC = wb[7], &dJK = wb[8], &dT1 = wb[10], &dT2 = wb[11], &dE = wb[12], &dW = wb[13],
             &dU = wb[14], &work = wb[15], &info = wb[16], &red = wb[17], &out = wb[18], &ring_F = wb[19],
             &ring_E = wb[20];
   // occupied eigenvectors (X basis), purification scalars, Cholesky infos
@@ -482,7 +484,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       (rc = ensure(ctx, dX, b_nn, "scf X")) || (rc = ensure(ctx, dF, b_nn, "scf F")) ||
       (rc = ensure(ctx, dFex, b_nn, "scf Fex")) || (rc = ensure(ctx, dD, b_nn, "scf D")) ||
       (rc = ensure(ctx, dDn, b_nn, "scf Dn")) || (rc = ensure(ctx, dC, b_nn, "scf C")) ||
-      (rc = ensure(ctx, dJ, b_nn, "scf J")) || (rc = ensure(ctx, dK, b_nn, "scf K")) ||
+      (rc = ensure(ctx, dJK, 2 * b_nn, "scf J, K")) ||
       (rc = ensure(ctx, dT1, b_nn, "scf T1")) || (rc = ensure(ctx, dT2, b_nn, "scf T2")) ||
       (rc = ensure(ctx, dE, b_nn, "scf E")) || (rc = ensure(ctx, dU, b_nn, "scf U")) ||
       (rc = ensure(ctx, dW, n * sizeof(double), "scf w")) || (rc = ensure(ctx, info, sizeof(int), "scf info")) ||
@@ -504,8 +506,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   double* pD = static_cast<double*>(dD.p);
   double* pDn = static_cast<double*>(dDn.p);
   double* pC = static_cast<double*>(dC.p);
-  double* pJ = static_cast<double*>(dJ.p);
-  double* pK = static_cast<double*>(dK.p);
+  double* pJ = static_cast<double*>(dJK.p);  // [J | K]: one array for the ranks' reduction
+  double* pK = pJ + nn;
   double* pT1 = static_cast<double*>(dT1.p);
   double* pT2 = static_cast<double*>(dT2.p);
   double* pU = static_cast<double*>(dU.p);
@@ -523,6 +525,13 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   auto fail = [&](int code, const char* msg) {
     cleanup();
     return set_err(ctx, code, "rijk_scf: %s", msg);
+  };
+  // the sum of the ranks' partial J and K (aux-sharded SCF), by the caller's collective
+  auto reduce_jk = [&]() -> int {
+    if (!o.reduce_jk) return RIJK_OK;
+    if (const int r = o.reduce_jk(pJ, 2 * nn, static_cast<void*>(s), o.reduce_user))
+      return set_err(ctx, RIJK_ERR_REDUCE, "rijk_scf: reduce_jk returned %d", r);
+    return cuda_check(ctx, cudaGetLastError(), "rijk_scf reduce_jk");
   };
   auto reduce = [&](auto f, long count, int is_max, int slot) {
     if (is_max)
@@ -716,6 +725,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     // The guess Fock matrix only seeds the first diagonalisation: a mixed run builds it in the
     // mixed form (the factor rows in orbital batches inside the build).
     rc = fock_device_impl(ctx, pD, static_cast<const double*>(dR.p), o.guess_nrows, pJ, pK, o.precision);
+    if (!rc) rc = reduce_jk();
     if (!rc) {
       k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
       rc = cuda_check(ctx, cudaStreamSynchronize(s), "rijk_scf guess");
@@ -742,6 +752,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
   int last_prec = -1;  // precision of the last build (pF, pJ, pK hold its result)
   auto build = [&](int p) -> int {
     int r = fock_device_impl(ctx, pD, pC, nocc, pJ, pK, p);
+    if (!r) r = reduce_jk();
     if (r) return r;
     k_fock<<<grid_of(nn), 256, 0, s>>>(pH, pJ, pK, nn, pF);
     ++nbuild;

@@ -7,10 +7,28 @@ B, the expensive part (n^2 naux / 2 doubles), is divided; the metric factor (nau
 n x n matrices are replicated.  Over NVLink the exchange is 2 n^2 doubles per build (55 MB at
 n = 1856), small next to the per-rank contraction.
 
+The SCF shards the same way: every rank runs rijk_scf on its slice with the same arguments, and after
+each Fock build the library hands the partial [J | K] (one device array) to a callback that sums it over
+the ranks; the rest of every iteration is replicated, and identical on every rank.
+
 The local builder is any object with the FockBuilder methods set_metric, set_aux_range, set_3c,
-fock_device / dm_to_f_transform_ri (nopt_b200.rijk.FockBuilder on the rank's GPU).
+fock_device / dm_to_f_transform_ri / scf (nopt_b200.rijk.FockBuilder on the rank's GPU).
 """
 import numpy as np
+
+
+class DeviceArray:
+    """float64 device memory at a raw pointer, as torch.as_tensor takes it without a copy (the CUDA
+    array interface, version 2: no stream attached; the caller orders the work)."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 2}
+
+
+def device_tensor(ptr, count, device):
+    import torch
+    return torch.as_tensor(DeviceArray(ptr, count), device=device)
 
 
 def aux_slices(naux, world):
@@ -78,3 +96,27 @@ class ShardedFockBuilder:
         self._allreduce(jk)
         out = jk.cpu().numpy()
         return out[0], out[1]
+
+    def scf(self, H, S, n_c, e_nuc, **kw):
+        """Aux-sharded RHF (rijk_scf on this rank's slice; keyword arguments as FockBuilder.scf).
+        After every Fock build the partial [J | K] is summed over the group in place: over NCCL by an
+        all-reduce enqueued on the build's own stream; over another backend through host memory (the
+        stream synchronised first).  Every rank must call this with the same arguments."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        nccl = self.dist.get_backend(self.group) == "nccl"
+
+        def reduce_jk(ptr, count, stream):
+            t = device_tensor(ptr, count, dev)
+            ext = torch.cuda.ExternalStream(stream, device=dev) if stream else torch.cuda.default_stream(dev)
+            if nccl:
+                with torch.cuda.stream(ext):
+                    self._allreduce(t)
+                return
+            ext.synchronize()
+            h = t.cpu()
+            self._allreduce(h)
+            t.copy_(h)
+            torch.cuda.current_stream(dev).synchronize()
+
+        return self.local.scf(H, S, n_c, e_nuc, reduce_jk=reduce_jk, **kw)

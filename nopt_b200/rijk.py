@@ -22,6 +22,7 @@ _LIB = None
 
 OK = 0
 ERR_ARG, ERR_STATE, ERR_CUDA, ERR_ALLOC, ERR_SOLVER, ERR_TIMEOUT, ERR_NUMERIC, ERR_CONVERGE = -1, -2, -3, -4, -5, -6, -7, -8
+ERR_REDUCE = -9
 METRIC_INVSQRT, METRIC_CHOLESKY = 0, 1
 LAYOUT_NOPT_FULL, LAYOUT_PACKED = 0, 1
 PREC_FP64, PREC_MIXED, PREC_FP64_TC = 0, 1, 2
@@ -62,6 +63,10 @@ def basis_t(basis):
                   xyz.ctypes.data_as(_dp), ex.ctypes.data_as(_dp), co.ctypes.data_as(_dp))
 
 
+# int reduce_jk(double* jk, long count, void* stream, void* user): the ranks' sum of [J | K] in place
+REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, _dp, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p)
+
+
 class ScfOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv_dm_rms", ctypes.c_double), ("precision", ctypes.c_int),
                 ("switch_diis_err", ctypes.c_double), ("diis_size", ctypes.c_int),
@@ -69,7 +74,8 @@ class ScfOpts(ctypes.Structure):
                 ("guess_dm", _dp), ("guess_rows", _dp), ("guess_nrows", ctypes.c_long),
                 ("converger", ctypes.c_int), ("conv_grad", ctypes.c_double), ("conv_energy", ctypes.c_double),
                 ("lbfgs_vectors", ctypes.c_int), ("density_by_eigenvectors", ctypes.c_int),
-                ("fp64_phase_precision", ctypes.c_int), ("ao_projector", _dp), ("n_proj", ctypes.c_long)]
+                ("fp64_phase_precision", ctypes.c_int), ("ao_projector", _dp), ("n_proj", ctypes.c_long),
+                ("reduce_jk", REDUCE_FN), ("reduce_user", ctypes.c_void_p)]
 
 
 class ScfResult(ctypes.Structure):
@@ -308,7 +314,7 @@ class FockBuilder:
 
     def scf(self, H, S, n_c, e_nuc, precision=PREC_FP64, conv_dm_rms=1e-10, switch_diis_err=1e-5, max_iter=100,
             diis_size=8, guess=None, diis_keep_on_switch=False, converger=CONV_DIIS, conv_grad=1e-7,
-            conv_energy=1e-10, lbfgs_vectors=0, purify=True, fp64_phase=PREC_FP64, projector=None):
+            conv_energy=1e-10, lbfgs_vectors=0, purify=True, fp64_phase=PREC_FP64, projector=None, reduce_jk=None):
         """RHF on the GPU (rijk_scf); guess = (D0, R) with D0 = R^T R (e.g. SystemIntegrals.sad()),
         None for the core-Hamiltonian start; converger CONV_DIIS, CONV_SOSCF (the reference's
         L-BFGS orbital rotations, converged on max|4 F_ai| < conv_grad or |dE| < conv_energy), or
@@ -318,6 +324,9 @@ class FockBuilder:
         fp64_phase=PREC_FP64_TC makes the builds after a mixed phase FP64_TC ones.  projector (n x n_proj)
         confines the orbitals to the span of its columns, e.g. the Cartesian->spherical map of a
         Cartesian orbital basis (ints.d5_projector), as the reference's D5 treatment.
+        reduce_jk(ptr, count, stream) sums the device array [J | K] (count doubles at ptr, written on
+        the CUDA stream `stream`) over the ranks of an aux-sharded SCF, in place; an exception in it
+        ends the SCF and is raised here (nopt_b200.parallel.ShardedFockBuilder.scf gives the NCCL one).
         Returns (E, MO rows, result dict)."""
         n = self.n
         o = ScfOpts(max_iter, conv_dm_rms, precision, switch_diis_err, diis_size, 1 if diis_keep_on_switch else 0,
@@ -331,10 +340,22 @@ class FockBuilder:
         if projector is not None:
             T = _c(projector)
             o.ao_projector, o.n_proj = _p(T), T.shape[1]
+        failure = []
+        if reduce_jk is not None:
+            def _cb(ptr, count, stream, user):
+                try:
+                    reduce_jk(ctypes.cast(ptr, ctypes.c_void_p).value, int(count), stream or 0)
+                    return 0
+                except BaseException as e:  # reported through RIJK_ERR_REDUCE, raised below
+                    failure.append(e)
+                    return 1
+            o.reduce_jk = REDUCE_FN(_cb)  # kept alive by `o` for the call
         r = ScfResult()
         MO = np.zeros((n, n))
         rc = lib().rijk_scf(self._h, _p(_c(H)), _p(_c(S)), int(n_c), float(e_nuc), ctypes.byref(o), _p(MO),
                             ctypes.byref(r))
+        if failure:
+            raise failure[0]
         if rc != ERR_CONVERGE:  # not converged: the result (converged = 0) and its trace are returned
             self._check(rc)
         out = {k: getattr(r, k) for k, _ in ScfResult._fields_ if not k.startswith("history")}
