@@ -75,8 +75,10 @@ typedef struct {
   double ms_setup_metric; /* last rijk_set_metric, device time                             */
   double ms_setup_3c;     /* last rijk_set_3c, device time (metric contraction included)   */
   double ms_last_fock;    /* last Fock build, device time                                   */
-  double ms_coulomb;      /* of which the Coulomb pair (w and J passes)                     */
-  double ms_exchange;     /* of which half-transform + K                                    */
+  double ms_coulomb;      /* from its start until J is complete (the w and J passes)        */
+  double ms_exchange;     /* from then until its end.  FP64 and FP64_TC builds run the
+                             Coulomb pair beside the half-transform, so there the exchange
+                             starts before J is complete; mixed builds run them in turn    */
   double flops_last_fock; /* algorithmic FLOPs of the last build                            */
   double bytes_last_fock; /* algorithmic HBM bytes of the last build                        */
   long n, naux, npad, ntile;

@@ -6,7 +6,8 @@
 //   J[e] = sum_Q B[Q][e] w_Q            (pass 2, Q split into nsplit ranges, partials
 //                                        summed while unpacking)
 // Both passes stream B once with 128-bit loads that bypass L1; reductions are warp
-// shuffles.  Algorithmic traffic: 2 * |B| bytes per build.
+// shuffles.  Algorithmic traffic: 2 * |B| bytes per build.  Both stride over their work, so a
+// capped grid (one or two CTAs per SM, beside the half-transform) covers all of it.
 #include <algorithm>
 
 #include <cuda_bf16.h>
@@ -17,46 +18,50 @@
 namespace rijk {
 
 constexpr int W_QB = 4;        // aux functions per CTA in pass 1 (reuses each Dt load)
-constexpr int W_THREADS = 512;
+constexpr int W_THREADS = 256;  // at most 16K registers a CTA: two fit beside two half-transform CTAs
 
+// SIDE: the instantiation run beside the half-transform (its own shared-memory carveout); the same code
+template <bool SIDE>
 __global__ void __launch_bounds__(W_THREADS) k_coulomb_w(const double* __restrict__ B, const double* __restrict__ Dt,
                                                           long naux, long tile_elems, double* __restrict__ w) {
-  const long q0 = static_cast<long>(blockIdx.x) * W_QB;
   const long n2 = tile_elems / 2;
   const double2* D2 = reinterpret_cast<const double2*>(Dt);
-  double acc[W_QB];
-#pragma unroll
-  for (int j = 0; j < W_QB; ++j) acc[j] = 0.0;
-  const double2* Bq[W_QB];
-#pragma unroll
-  for (int j = 0; j < W_QB; ++j) {
-    long q = q0 + j < naux ? q0 + j : naux - 1;
-    Bq[j] = reinterpret_cast<const double2*>(B + q * tile_elems);
-  }
-  for (long e = threadIdx.x; e < n2; e += W_THREADS) {
-    double2 d = D2[e];
-#pragma unroll
-    for (int j = 0; j < W_QB; ++j) {
-      double2 b = ldg_stream(Bq[j] + e);
-      acc[j] = fma(b.x, d.x, acc[j]);
-      acc[j] = fma(b.y, d.y, acc[j]);
-    }
-  }
   __shared__ double red[W_QB][W_THREADS / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long q0 = static_cast<long>(blockIdx.x) * W_QB; q0 < naux; q0 += static_cast<long>(gridDim.x) * W_QB) {
+    double acc[W_QB];
 #pragma unroll
-  for (int j = 0; j < W_QB; ++j) {
-    double v = warp_sum(acc[j]);
-    if (lane == 0) red[j][warp] = v;
-  }
-  __syncthreads();
-  if (warp == 0) {
+    for (int j = 0; j < W_QB; ++j) acc[j] = 0.0;
+    const double2* Bq[W_QB];
 #pragma unroll
     for (int j = 0; j < W_QB; ++j) {
-      double v = lane < W_THREADS / 32 ? red[j][lane] : 0.0;
-      v = warp_sum(v);
-      if (lane == 0 && q0 + j < naux) w[q0 + j] = v;
+      long q = q0 + j < naux ? q0 + j : naux - 1;
+      Bq[j] = reinterpret_cast<const double2*>(B + q * tile_elems);
     }
+    for (long e = threadIdx.x; e < n2; e += W_THREADS) {
+      double2 d = D2[e];
+#pragma unroll
+      for (int j = 0; j < W_QB; ++j) {
+        double2 b = ldg_stream(Bq[j] + e);
+        acc[j] = fma(b.x, d.x, acc[j]);
+        acc[j] = fma(b.y, d.y, acc[j]);
+      }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < W_QB; ++j) {
+      double v = warp_sum(acc[j]);
+      if (lane == 0) red[j][warp] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+      for (int j = 0; j < W_QB; ++j) {
+        double v = lane < W_THREADS / 32 ? red[j][lane] : 0.0;
+        v = warp_sum(v);
+        if (lane == 0 && q0 + j < naux) w[q0 + j] = v;
+      }
+    }
+    __syncthreads();  // red is refilled by the next group of aux functions
   }
 }
 
@@ -64,36 +69,38 @@ constexpr int J_THREADS = 256;
 constexpr int J_UNROLL = 4;
 
 // Jpart[s][e] = sum_{Q in split s} B[Q][e] w[Q]; each thread owns one double2 of e.
+template <bool SIDE>
 __global__ void __launch_bounds__(J_THREADS) k_coulomb_j(const double* __restrict__ B, const double* __restrict__ w,
                                                           long naux, long tile_elems, long qper,
                                                           double* __restrict__ Jpart) {
-  const long e2 = static_cast<long>(blockIdx.x) * J_THREADS + threadIdx.x;
   const long s = blockIdx.y;
   const long qa = s * qper;
   const long qb = qa + qper < naux ? qa + qper : naux;
-  if (e2 * 2 >= tile_elems) return;
-  const double2* Bp = reinterpret_cast<const double2*>(B) + e2;
   const long stride2 = tile_elems / 2;
-  double ax = 0.0, ay = 0.0;
-  long q = qa;
-  for (; q + J_UNROLL <= qb; q += J_UNROLL) {
-    double2 b[J_UNROLL];
+  for (long e2 = static_cast<long>(blockIdx.x) * J_THREADS + threadIdx.x; e2 < stride2;
+       e2 += static_cast<long>(gridDim.x) * J_THREADS) {
+    const double2* Bp = reinterpret_cast<const double2*>(B) + e2;
+    double ax = 0.0, ay = 0.0;
+    long q = qa;
+    for (; q + J_UNROLL <= qb; q += J_UNROLL) {
+      double2 b[J_UNROLL];
 #pragma unroll
-    for (int u = 0; u < J_UNROLL; ++u) b[u] = ldg_stream(Bp + (q + u) * stride2);
+      for (int u = 0; u < J_UNROLL; ++u) b[u] = ldg_stream(Bp + (q + u) * stride2);
 #pragma unroll
-    for (int u = 0; u < J_UNROLL; ++u) {
-      double wq = __ldg(w + q + u);
-      ax = fma(b[u].x, wq, ax);
-      ay = fma(b[u].y, wq, ay);
+      for (int u = 0; u < J_UNROLL; ++u) {
+        double wq = __ldg(w + q + u);
+        ax = fma(b[u].x, wq, ax);
+        ay = fma(b[u].y, wq, ay);
+      }
     }
+    for (; q < qb; ++q) {
+      double2 b = ldg_stream(Bp + q * stride2);
+      double wq = __ldg(w + q);
+      ax = fma(b.x, wq, ax);
+      ay = fma(b.y, wq, ay);
+    }
+    reinterpret_cast<double2*>(Jpart + s * tile_elems)[e2] = make_double2(ax, ay);
   }
-  for (; q < qb; ++q) {
-    double2 b = ldg_stream(Bp + q * stride2);
-    double wq = __ldg(w + q);
-    ax = fma(b.x, wq, ax);
-    ay = fma(b.y, wq, ay);
-  }
-  reinterpret_cast<double2*>(Jpart + s * tile_elems)[e2] = make_double2(ax, ay);
 }
 
 int coulomb_nsplit(long tile_elems, long naux, int elems_per_thread) {
@@ -105,23 +112,49 @@ int coulomb_nsplit(long tile_elems, long naux, int elems_per_thread) {
   return static_cast<int>(want);
 }
 
-void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s) {
-  unsigned grid = static_cast<unsigned>((naux + W_QB - 1) / W_QB);
-  k_coulomb_w<<<grid, W_THREADS, 0, s>>>(B, Dt, naux, tile_elems, w);
+// The capped forms ask for the largest shared-memory carveout, the one the half-transform runs with, so that
+// their CTAs can share its SMs.  The forms run alone keep the default (their L1 caches w and Dt).
+static void prefer_shared_carveout() {
+  static const bool once = [] {
+    cudaFuncSetAttribute(k_coulomb_w<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(k_coulomb_j<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    return true;
+  }();
+  (void)once;
+}
+
+void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s,
+                      int max_ctas) {
+  long grid = (naux + W_QB - 1) / W_QB;
+  if (max_ctas > 0) {
+    prefer_shared_carveout();
+    if (grid > max_ctas) grid = max_ctas;
+    k_coulomb_w<true><<<static_cast<unsigned>(grid), W_THREADS, 0, s>>>(B, Dt, naux, tile_elems, w);
+    return;
+  }
+  k_coulomb_w<false><<<static_cast<unsigned>(grid), W_THREADS, 0, s>>>(B, Dt, naux, tile_elems, w);
 }
 
 cudaError_t preload_coulomb_kernels() {
   cudaFuncAttributes a;
-  cudaError_t e = cudaFuncGetAttributes(&a, k_coulomb_w);
-  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_coulomb_j);
+  cudaError_t e = cudaFuncGetAttributes(&a, k_coulomb_w<false>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_coulomb_j<false>);
   return e;
 }
 
 void launch_coulomb_j(const double* B, const double* w, long naux, long tile_elems, int nsplit, double* Jpart,
-                      cudaStream_t s) {
+                      cudaStream_t s, int max_ctas) {
+  if (max_ctas > 0) prefer_shared_carveout();
   long qper = (naux + nsplit - 1) / nsplit;
-  dim3 grid(static_cast<unsigned>((tile_elems / 2 + J_THREADS - 1) / J_THREADS), static_cast<unsigned>(nsplit));
-  k_coulomb_j<<<grid, J_THREADS, 0, s>>>(B, w, naux, tile_elems, qper, Jpart);
+  long gx = (tile_elems / 2 + J_THREADS - 1) / J_THREADS;
+  if (max_ctas > 0 && gx * nsplit > max_ctas) gx = std::max<long>(1, max_ctas / nsplit);
+  dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(nsplit));
+  if (max_ctas > 0)
+    k_coulomb_j<true><<<grid, J_THREADS, 0, s>>>(B, w, naux, tile_elems, qper, Jpart);
+  else
+    k_coulomb_j<false><<<grid, J_THREADS, 0, s>>>(B, w, naux, tile_elems, qper, Jpart);
 }
 
 // ---------------------------------------------------------------------------------

@@ -133,6 +133,14 @@ cudaError_t preload_density_kernels() {
   return e;
 }
 
+// Ends after `cycles` SM clock cycles, whatever happens elsewhere: it waits on nothing.
+__global__ void k_delay(long long cycles) {
+  const long long t0 = clock64();
+  while (clock64() - t0 < cycles) __nanosleep(500);
+}
+
+void launch_delay(long long cycles, cudaStream_t s) { k_delay<<<1, 32, 0, s>>>(cycles); }
+
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s) {
   k_pack_mo<<<grid_for(noccp * npad, 256), 256, 0, s>>>(MO, nocc, n, noccp, npad, MOp);
 }

@@ -202,11 +202,30 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
       (rc = ensure(ctx, ctx->Jpart, static_cast<size_t>(nsJ) * tile_elems * sizeof(double), "Jpart")))
     return rc;
   if (precision == RIJK_PREC_MIXED && (rc = mixed_prepare(ctx))) return rc;
+  // FP64 and FP64_TC: the Coulomb pair runs on the high-priority stream beside the half-transform, two
+  // 256-thread CTAs per SM, in the registers and warps the half-transform's two CTAs per SM leave free;
+  // the pair is bound by HBM, the half-transform by the FP64 tensor pipe.  With per-kernel timing on,
+  // the kernels run one after another instead.
+  const bool side_j = precision != RIJK_PREC_MIXED && nocc > 0 && !ctx->profiling;
   cudaEventRecord(ctx->ev0, s);
   prof_begin(ctx);
   launch_pack_density(dD, n, npad, nt, static_cast<double*>(ctx->Dt.p), s);
   prof_mark(ctx, "pack_density");
-  if (precision == RIJK_PREC_MIXED) {
+  if (side_j) {
+    cudaStream_t js = ctx->j_stream;
+    cudaEventRecord(ctx->ev_pk, s);
+    cudaStreamWaitEvent(js, ctx->ev_pk, 0);
+    launch_coulomb_w(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->Dt.p), naux, tile_elems,
+                     static_cast<double*>(ctx->w.p), js, 2 * ctx->sms);
+    // the same aux ranges as the pass run alone, so J's sums are the same
+    launch_coulomb_j(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->w.p), naux, tile_elems, nsJ,
+                     static_cast<double*>(ctx->Jpart.p), js, 2 * ctx->sms);
+    launch_unpack_sym(static_cast<double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, js);
+    launches += 4 + (nsJ > 1 ? 1 : 0);  // pack, w, j, unpack (+ split sum)
+    cudaEventRecord(ctx->ev1, js);
+    if (j_done) cudaEventRecord(j_done, js);
+    cudaEventRecord(ctx->ev_jside, js);
+  } else if (precision == RIJK_PREC_MIXED) {
     // mixed form: both passes over the split-BF16 copy (half the bytes of the FP64 passes)
     const long ntile2 = round_up(nt, 2) * (round_up(nt, 2) + 1) / 2;
     const __nv_bfloat16* Bm = static_cast<const __nv_bfloat16*>(ctx->Bmix.p);
@@ -224,11 +243,13 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
                      nsJ, static_cast<double*>(ctx->Jpart.p), s);
     prof_mark(ctx, "coulomb_j");
   }
-  launch_unpack_sym(static_cast<double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, s);
-  prof_mark(ctx, "unpack_j");
-  launches += (precision == RIJK_PREC_MIXED ? 5 : 4) + (nsJ > 1 ? 1 : 0);  // pack, w (+ chunk sum), j, unpack (+ split sum)
-  cudaEventRecord(ctx->ev1, s);
-  if (j_done) cudaEventRecord(j_done, s);
+  if (!side_j) {
+    launch_unpack_sym(static_cast<double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, s);
+    prof_mark(ctx, "unpack_j");
+    launches += (precision == RIJK_PREC_MIXED ? 5 : 4) + (nsJ > 1 ? 1 : 0);  // pack, w (+ chunk sum), j, unpack (+ split sum)
+    cudaEventRecord(ctx->ev1, s);
+    if (j_done) cudaEventRecord(j_done, s);
+  }
   if (mo_ready && nocc > 0) cudaStreamWaitEvent(s, mo_ready, 0);
 
   if (nocc == 0) {
@@ -247,6 +268,13 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
         (rc = ensure(ctx, ctx->XT, static_cast<size_t>(npad) * kdim * sizeof(double), "XT")) ||
         (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(nsK) * tile_elems * sizeof(double), "Kpart")))
       return rc;
+    // About 20 us, so that the Coulomb CTAs, whose stream waits on an event, are resident before the
+    // half-transform's thousands of CTAs queue (builds queued back to back: 240.5 -> 235.2 ms at
+    // n_ao = 1856, where the pair alone takes 17.7 ms)
+    if (side_j) {
+      launch_delay(40000, s);
+      ++launches;
+    }
     launch_pack_mo(dMO, nocc, n, noccp, npad, static_cast<double*>(ctx->MOp.p), s);
     prof_mark(ctx, "pack_mo");
     launches += launch_xform_f64(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->MOp.p), naux,
@@ -267,6 +295,7 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
     prof_mark(ctx, "unpack_k");
     launches += 3 + (nsK > 1 ? 1 : 0);  // pack_mo, syrk, unpack (+ split sum); the half-transform counted above
   }
+  if (side_j) cudaStreamWaitEvent(s, ctx->ev_jside, 0);  // J joins the build's stream
   cudaEventRecord(ctx->ev2, s);
   rc = cuda_check(ctx, cudaGetLastError(), "fock launch");
   if (rc) return rc;
@@ -308,6 +337,18 @@ RIJK_API int rijk_create(rijk_ctx** out, int device) {
   }
   cudaEventCreateWithFlags(&ctx->ev_mo, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ctx->ev_j, cudaEventDisableTiming);
+  {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (cudaStreamCreateWithPriority(&ctx->j_stream, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+      rijk_destroy(ctx);
+      return RIJK_ERR_CUDA;
+    }
+  }
+  cudaEventCreateWithFlags(&ctx->ev_pk, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ctx->ev_jside, cudaEventDisableTiming);
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  if (ctx->sms <= 0) ctx->sms = 148;
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
   cudaEventCreate(&ctx->ev2);
@@ -337,6 +378,7 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // before any buffer it may touch is freed
+  if (ctx->j_stream) cudaStreamSynchronize(ctx->j_stream);
   DeviceBuf* bufs[] = {&ctx->M,  &ctx->B,     &ctx->Bmix,  &ctx->stageD, &ctx->stageMO, &ctx->stageJ,
                        &ctx->stageK, &ctx->Dt, &ctx->w,     &ctx->Jpart, &ctx->MOp,    &ctx->XT,
                        &ctx->Kpart, &ctx->err, &ctx->scratch, &ctx->eri_tab, &ctx->Xs, &ctx->Xe,
@@ -349,7 +391,8 @@ RIJK_API int rijk_destroy(rijk_ctx* ctx) {
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);
   }
-  cudaEvent_t evs[] = {ctx->ev0, ctx->ev1, ctx->ev2, ctx->ev3, ctx->ev_mo, ctx->ev_j};
+  if (ctx->j_stream) cudaStreamDestroy(ctx->j_stream);
+  cudaEvent_t evs[] = {ctx->ev0, ctx->ev1, ctx->ev2, ctx->ev3, ctx->ev_mo, ctx->ev_j, ctx->ev_pk, ctx->ev_jside};
   for (cudaEvent_t ev : evs)
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : ctx->pev)

@@ -64,6 +64,11 @@ struct rijk_ctx {
   // the Coulomb and exchange kernels run
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_mo = nullptr, ev_j = nullptr;
+  // FP64 builds: the Coulomb pair runs on a high-priority stream beside the half-transform, in the
+  // registers and shared memory its CTAs leave free on every SM (joined before the build ends)
+  cudaStream_t j_stream = nullptr;
+  cudaEvent_t ev_pk = nullptr, ev_jside = nullptr;
+  int sms = 148;
 
   long n = 0, naux = 0, npad = 0, nt = 0, ntile = 0;
   long q0 = 0, nq = 0;  // aux functions [q0, q0 + nq) held in B (all of them unless rijk_set_aux_range)
@@ -194,6 +199,8 @@ void gemm_f64(const GemmF64Args& p, long batch, cudaStream_t s);
 cudaError_t preload_density_kernels();
 void launch_pack_density(const double* D, long n, long npad, long nt, double* Dt, cudaStream_t s);
 void launch_pack_mo(const double* MO, long nocc, long n, long noccp, long npad, double* MOp, cudaStream_t s);
+// One warp that sleeps for `cycles` SM clock cycles and exits (a fixed delay on a stream).
+void launch_delay(long long cycles, cudaStream_t s);
 void launch_unpack_sym(double* partial, int nsplit, long ntile, long n, double* out, cudaStream_t s);
 void launch_unpack_sym_f32(const float* partial, int nsplit, long ntile, long n, double* sum, double* out,
                            cudaStream_t s);
@@ -214,9 +221,11 @@ cudaError_t preload_coulomb_kernels();
 int coulomb_nsplit(long tile_elems, long naux, int elems_per_thread);
 // Octet chunks of the mixed w pass; its w buffer holds (1 + chunks) * naux doubles.
 int coulomb_w_mixed_chunks(long ntile);
-void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s);
+// max_ctas > 0 caps the grid (the kernels stride over the rest), for the pair run beside the half-transform
+void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s,
+                      int max_ctas = 0);
 void launch_coulomb_j(const double* B, const double* w, long naux, long tile_elems, int nsplit, double* Jpart,
-                      cudaStream_t s);
+                      cudaStream_t s, int max_ctas = 0);
 
 // Mixed form: the same passes over the split-BF16 copy (Bmix[Q][t][hl][64][64], ntile2 tiles per Q).
 void launch_coulomb_w_mixed(const __nv_bfloat16* Bmix, const double* Dt, long naux, long ntile, long ntile2, double* w,
