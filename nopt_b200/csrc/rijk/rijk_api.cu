@@ -202,8 +202,8 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
       (rc = ensure(ctx, ctx->Jpart, static_cast<size_t>(nsJ) * tile_elems * sizeof(double), "Jpart")))
     return rc;
   if (precision == RIJK_PREC_MIXED && (rc = mixed_prepare(ctx))) return rc;
-  // FP64 and FP64_TC: the Coulomb pair runs on the high-priority stream beside the half-transform, two
-  // 256-thread CTAs per SM, in the registers and warps the half-transform's two CTAs per SM leave free;
+  // FP64 and FP64_TC: the Coulomb pair runs on the high-priority stream beside the half-transform, one
+  // 256-thread CTA per SM, in the registers and warps the half-transform's two CTAs per SM leave free;
   // the pair is bound by HBM, the half-transform by the FP64 tensor pipe.  With per-kernel timing on,
   // the kernels run one after another instead.
   const bool side_j = precision != RIJK_PREC_MIXED && nocc > 0 && !ctx->profiling;
@@ -216,10 +216,10 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
     cudaEventRecord(ctx->ev_pk, s);
     cudaStreamWaitEvent(js, ctx->ev_pk, 0);
     launch_coulomb_w(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->Dt.p), naux, tile_elems,
-                     static_cast<double*>(ctx->w.p), js, 2 * ctx->sms);
+                     static_cast<double*>(ctx->w.p), js, ctx->sms);
     // the same aux ranges as the pass run alone, so J's sums are the same
     launch_coulomb_j(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->w.p), naux, tile_elems, nsJ,
-                     static_cast<double*>(ctx->Jpart.p), js, 2 * ctx->sms);
+                     static_cast<double*>(ctx->Jpart.p), js, ctx->sms);
     launch_unpack_sym(static_cast<double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, js);
     launches += 4 + (nsJ > 1 ? 1 : 0);  // pack, w, j, unpack (+ split sum)
     cudaEventRecord(ctx->ev1, js);

@@ -90,6 +90,23 @@ def test_jk_parity_water_hexamer_jkfit():
     assert np.max(np.abs(K - Kr)) < TOL_JK
 
 
+@pytest.mark.parametrize("precision", [rijk.PREC_FP64, rijk.PREC_FP64_TC])
+def test_two_stream_build_equals_one_stream_build(precision):
+    """FP64 builds run the Coulomb pair on a second stream beside the half-transform, with capped grids
+    that stride over the work; with per-kernel timing on, every kernel runs alone on full grids.  Each aux
+    function's w and each element's J are summed in the same order either way: J and K are identical."""
+    si = ints.SystemIntegrals(water_cluster((2, 3), seed=0), "cc-pvdz", "cc-pvdz-jkfit")
+    DM, MO = _random_state(si.n, si.nocc, 5)
+    with rijk.FockBuilder(0) as fb:
+        fb.set_metric(si.V)
+        fb.set_3c(si.I3, si.n)
+        J2, K2 = fb.dm_to_f_transform_ri(DM, MO, si.nocc, precision)
+        fb.set_profiling(True)
+        J1, K1 = fb.dm_to_f_transform_ri(DM, MO, si.nocc, precision)
+        assert fb.stats()["profiled_stages"] > 0
+    assert np.array_equal(J1, J2) and np.array_equal(K1, K2)
+
+
 def _random_problem(n, naux, seed):
     rng = np.random.default_rng(seed)
     A = rng.normal(size=(naux, naux))
