@@ -52,6 +52,7 @@ int ensure(rijk_ctx* ctx, DeviceBuf& b, size_t bytes, const char* what) {
   if (b.p) {  // the old buffer may still be read by work queued on the context's streams
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    if (ctx->j_stream) cudaStreamSynchronize(ctx->j_stream);
     cudaFree(b.p);
   }
   b.p = nullptr;
@@ -202,6 +203,19 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
       (rc = ensure(ctx, ctx->Jpart, static_cast<size_t>(nsJ) * tile_elems * sizeof(double), "Jpart")))
     return rc;
   if (precision == RIJK_PREC_MIXED && (rc = mixed_prepare(ctx))) return rc;
+  // the FP64 exchange's buffers, before anything is queued: growing one drains the streams
+  const long noccp = round_up(nocc, 16);
+  const long kdim = naux * noccp;
+  const bool tc = precision == RIJK_PREC_FP64_TC;
+  long kper_tc = 0;
+  int nsK = 1;
+  if (nocc > 0 && precision != RIJK_PREC_MIXED) {
+    nsK = tc ? syrk_i8_parts(nt, kdim, ctx->device, &kper_tc) : syrk_nsplit(nt, kdim);
+    if ((rc = ensure(ctx, ctx->MOp, noccp * npad * sizeof(double), "MOp")) ||
+        (rc = ensure(ctx, ctx->XT, static_cast<size_t>(npad) * kdim * sizeof(double), "XT")) ||
+        (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(nsK) * tile_elems * sizeof(double), "Kpart")))
+      return rc;
+  }
   // FP64 and FP64_TC: the Coulomb pair runs on the high-priority stream beside the half-transform, one
   // 256-thread CTA per SM, in the registers and warps the half-transform's two CTAs per SM leave free;
   // the pair is bound by HBM, the half-transform by the FP64 tensor pipe.  With per-kernel timing on,
@@ -259,15 +273,6 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
     if (rc) return rc;
     launches += ctx->stats.kernels_last_fock;
   } else {
-    const long noccp = round_up(nocc, 16);
-    const long kdim = naux * noccp;
-    const bool tc = precision == RIJK_PREC_FP64_TC;
-    long kper_tc = 0;
-    const int nsK = tc ? syrk_i8_parts(nt, kdim, ctx->device, &kper_tc) : syrk_nsplit(nt, kdim);
-    if ((rc = ensure(ctx, ctx->MOp, noccp * npad * sizeof(double), "MOp")) ||
-        (rc = ensure(ctx, ctx->XT, static_cast<size_t>(npad) * kdim * sizeof(double), "XT")) ||
-        (rc = ensure(ctx, ctx->Kpart, static_cast<size_t>(nsK) * tile_elems * sizeof(double), "Kpart")))
-      return rc;
     // About 20 us, so that the Coulomb CTAs, whose stream waits on an event, are resident before the
     // half-transform's thousands of CTAs queue (builds queued back to back: 240.5 -> 235.2 ms at
     // n_ao = 1856, where the pair alone takes 17.7 ms)
@@ -283,7 +288,10 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
     if (tc) {  // int8 digit planes of X^T, then K on tcgen05 (exact s32 products)
       rc = syrk_i8(ctx, static_cast<const double*>(ctx->XT.p), npad, nt, kdim, nsK, kper_tc,
                    static_cast<double*>(ctx->Kpart.p), s);
-      if (rc) return rc;
+      if (rc) {
+        if (side_j) cudaStreamWaitEvent(s, ctx->ev_jside, 0);  // nothing of the side stream outlives the call
+        return rc;
+      }
       prof_mark(ctx, "syrk_i8");
       ++launches;  // the digit-plane pass
     } else {

@@ -20,7 +20,7 @@ def _pin(name):
     return ints.SystemIntegrals(Molecule(p["symbols"], p["coords_ang"]), p["basis"], p["aux"]), p
 
 
-@pytest.mark.parametrize("name", ["c2h4", "guanine"])
+@pytest.mark.parametrize("name", ["c2h4", "c6h8", "guanine"])
 def test_gpu_scf_reproduces_reference_energy(name):
     si, p = _pin(name)
     with rijk.FockBuilder(0) as fb:
