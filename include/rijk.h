@@ -101,10 +101,14 @@ typedef struct {
 
 int rijk_create(rijk_ctx** ctx, int device);
 int rijk_destroy(rijk_ctx* ctx);
-/* Run on the caller's CUDA stream (a cudaStream_t) instead of the context's own. */
+/* Run on the caller's CUDA stream (a cudaStream_t) instead of the context's own.  An FP64 or FP64_TC
+ * build also runs its Coulomb passes on a second stream the context owns: that stream waits on the
+ * caller's stream at the start of the build, and the caller's stream waits on it before the build's
+ * end, so work queued after the build on the caller's stream sees J and K. */
 int rijk_set_stream(rijk_ctx* ctx, void* stream);
 int rijk_last_error(const rijk_ctx* ctx, char* buf, int len);
-/* Record a CUDA event around every kernel of a Fock build (for per-kernel timing). */
+/* Record a CUDA event around every kernel of a Fock build (for per-kernel timing); the kernels then
+ * run one after another on one stream. */
 int rijk_set_profiling(rijk_ctx* ctx, int on);
 int rijk_get_stats(const rijk_ctx* ctx, rijk_stats_t* out);
 
