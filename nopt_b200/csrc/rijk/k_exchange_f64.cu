@@ -20,6 +20,39 @@ namespace rijk {
 
 constexpr int X_THREADS = 128;
 
+// The half-transform's [row][k] chunks (the K-major tiles of B^Q and the orbitals) without padding: the
+// 8-byte words of a row are XOR-swizzled, (row, k) at row * 32 + (k ^ 4 (row & 3)).  A half-warp reads
+// rows g = 0..3 (or 4..7) at k + t, t = 0..3, and the swizzle spreads those over 16 distinct words mod 16,
+// as the padded stride 36 did.  Every fragment row is g plus a multiple of 4, so the swizzle is one
+// per-lane constant: (k + t) ^ 4 (g & 3) = (k ^ 4 (g & 3)) + t.  The XOR keeps pairs of words together,
+// so each 16-byte copy stays whole and aligned.  The [k][row] chunks keep the padded stride 68.
+// 74 KB of stages a CTA at 80 orbitals instead of 81 KB: three CTAs share an SM instead of two.
+constexpr int XK = 32;  // [row][k] row length
+__device__ __forceinline__ int swk(int row, int k) { return row * XK + (k ^ ((row & 3) << 2)); }
+
+// warp_mma_chunk with the swizzled [row][k] chunks; m0 and n0 are multiples of 4
+template <int MF, int NF, bool A_KMAJOR>
+__device__ __forceinline__ void warp_mma_chunk_sw(double (&acc)[MF][NF][2], const double* __restrict__ sA,
+                                                  const double* __restrict__ sB, int m0, int n0, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int sg = (g & 3) << 2;
+  const double* pa = A_KMAJOR ? sA + (m0 + g) * XK + t : sA + t * LDM + m0 + g;
+  const double* pb = sB + (n0 + g) * XK + t;
+#pragma unroll
+  for (int k = 0; k < KC; k += 4) {
+    const int kx = k ^ sg;
+    double a[MF], b[NF];
+#pragma unroll
+    for (int i = 0; i < MF; ++i) a[i] = A_KMAJOR ? pa[i * 8 * XK + kx] : pa[k * LDM + i * 8];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) b[j] = pb[j * 8 * XK + kx];
+#pragma unroll
+    for (int i = 0; i < MF; ++i)
+#pragma unroll
+      for (int j = 0; j < NF; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+  }
+}
+
 // Grid (nb * nt, naux): block x = J nb + b handles orbital batch b (rows i0 + b NOCCP of MOp) of tile
 // column J, so the nb batches of one (J, Q) run back to back and the later ones read the tiles of B^Q
 // from L2.
@@ -28,8 +61,9 @@ __global__ void __launch_bounds__(X_THREADS)
     k_xform_f64(const double* __restrict__ B, const double* __restrict__ MOp_all, long nt, long npad, long tile_elems,
                 long kdim, long noccp_total, long i0_first, int nb, double* __restrict__ XT) {
   constexpr int NOCCP = NF * 16;
-  constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
-  constexpr int B_STAGE = NOCCP * LDK;
+  constexpr int A_STAGE = (64 * XK > KC * LDM) ? 64 * XK : KC * LDM;
+  constexpr int B_STAGE = NOCCP * XK;
+  static_assert(KC == XK, "chunk shape");
   extern __shared__ __align__(16) double smem[];
   double* sA[2] = {smem, smem + A_STAGE};
   double* sB[2] = {smem + 2 * A_STAGE, smem + 2 * A_STAGE + B_STAGE};
@@ -51,7 +85,7 @@ __global__ void __launch_bounds__(X_THREADS)
       for (int it = 0; it < 8; ++it) {
         int idx = tid + it * X_THREADS;
         int row = idx >> 4, seg = idx & 15;
-        cp_async16(&sA[stage][row * LDK + seg * 2], tp + row * TILE + seg * 2, true);
+        cp_async16(&sA[stage][swk(row, seg * 2)], tp + row * TILE + seg * 2, true);
       }
     } else {  // tile (I, J): rows mu, cols nu -> [mu-chunk][nu]
       const double* tp = BQ + tri_index(I, J) * TILE2 + half * KC * TILE;
@@ -65,7 +99,7 @@ __global__ void __launch_bounds__(X_THREADS)
     const double* cp = MOp + I * TILE + half * KC;
     for (int idx = tid; idx < NOCCP * 16; idx += X_THREADS) {
       int row = idx >> 4, seg = idx & 15;
-      cp_async16(&sB[stage][row * LDK + seg * 2], cp + row * npad + seg * 2, true);
+      cp_async16(&sB[stage][swk(row, seg * 2)], cp + row * npad + seg * 2, true);
     }
   };
 
@@ -84,9 +118,9 @@ __global__ void __launch_bounds__(X_THREADS)
     }
     __syncthreads();
     if (J >= (kc >> 1))
-      warp_mma_chunk<4, NF, true>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * (NOCCP / 2), lane);
+      warp_mma_chunk_sw<4, NF, true>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * (NOCCP / 2), lane);
     else
-      warp_mma_chunk<4, NF, false>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * (NOCCP / 2), lane);
+      warp_mma_chunk_sw<4, NF, false>(acc, sA[kc & 1], sB[kc & 1], wm * 32, wn * (NOCCP / 2), lane);
     __syncthreads();
   }
 
@@ -106,9 +140,15 @@ template <int NF>
 static void launch_xform_nf(const double* B, const double* MOp, long naux, long nt, long noccp_total, long i0, int nb,
                             double* XT, cudaStream_t s) {
   constexpr int NOCCP = NF * 16;
-  constexpr int A_STAGE = (64 * LDK > KC * LDM) ? 64 * LDK : KC * LDM;
-  size_t smem = (2 * A_STAGE + 2 * NOCCP * LDK) * sizeof(double);
+  constexpr int A_STAGE = (64 * XK > KC * LDM) ? 64 * XK : KC * LDM;
+  size_t smem = (2 * A_STAGE + 2 * NOCCP * XK) * sizeof(double);
   ensure_smem_limit(reinterpret_cast<const void*>(k_xform_f64<NF>), smem);
+  static const bool carveout = [] {  // room for three CTAs an SM
+    cudaFuncSetAttribute(k_xform_f64<NF>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    return true;
+  }();
+  (void)carveout;
   long npad = nt * TILE;
   long tile_elems = nt * (nt + 1) / 2 * TILE2;
   dim3 grid(static_cast<unsigned>(nt * nb), static_cast<unsigned>(naux));
