@@ -225,15 +225,18 @@ int fock_device_impl(rijk_ctx* ctx, const double* dD, const double* dMO, long no
   prof_begin(ctx);
   launch_pack_density(dD, n, npad, nt, static_cast<double*>(ctx->Dt.p), s);
   prof_mark(ctx, "pack_density");
+  // The pair's CTAs (one or two an SM): the half-transform's time per byte of B grows with the orbitals,
+  // so fewer orbitals leave a shorter window for the same bytes
+  const int side_ctas = noccp <= 96 ? 2 * ctx->sms : ctx->sms;
   if (side_j) {
     cudaStream_t js = ctx->j_stream;
     cudaEventRecord(ctx->ev_pk, s);
     cudaStreamWaitEvent(js, ctx->ev_pk, 0);
     launch_coulomb_w(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->Dt.p), naux, tile_elems,
-                     static_cast<double*>(ctx->w.p), js, ctx->sms);
+                     static_cast<double*>(ctx->w.p), js, side_ctas);
     // the same aux ranges as the pass run alone, so J's sums are the same
     launch_coulomb_j(static_cast<const double*>(ctx->B.p), static_cast<const double*>(ctx->w.p), naux, tile_elems, nsJ,
-                     static_cast<double*>(ctx->Jpart.p), js, ctx->sms);
+                     static_cast<double*>(ctx->Jpart.p), js, side_ctas);
     launch_unpack_sym(static_cast<double*>(ctx->Jpart.p), nsJ, ntile, n, dJ, js);
     launches += 4 + (nsJ > 1 ? 1 : 0);  // pack, w, j, unpack (+ split sum)
     cudaEventRecord(ctx->ev1, js);
