@@ -43,9 +43,9 @@ NCU_TRAFFIC = {("h2o16_dz", "xform_f64"): 1.277529e9 + 0.437618e9,
                ("h2o16_dz", "coulomb_w_mixed"): 0.639341e9 + 0.004234e9,
                ("h2o16_dz", "coulomb_j_mixed"): 0.638610e9 + 0.010762e9,
                # (H2O)32 cc-pVTZ: the half-transform captured on a synthetic case with its orbital shape and
-               # 256 aux functions (one launch, both 80-orbital batches: 3.943e9 read + 0.658e9 written),
+               # 256 aux functions (one launch, both 80-orbital batches: 4.469e9 read + 0.653e9 written),
                # scaled by aux functions (4448)
-               ("h2o32_tz", "xform_f64"): (3.942770e9 + 0.658444e9) / 256 * 4448}
+               ("h2o32_tz", "xform_f64"): (4.469058e9 + 0.652858e9) / 256 * 4448}
 WORKLOAD_NAMES = {"h2o6_dz": "(H2O)6 cc-pVDZ/cc-pVDZ-JKFIT", "h2o16_dz": "(H2O)16 cc-pVDZ/cc-pVDZ-JKFIT",
                   "c40h82_dz": "C40H82 cc-pVDZ/cc-pVDZ-JKFIT", "h2o32_tz": "(H2O)32 cc-pVTZ/cc-pVTZ-JKFIT"}
 METRIC = "RI-JK Fock builds/s (FP64 drop-in; mixed and SCF time beside it)"
