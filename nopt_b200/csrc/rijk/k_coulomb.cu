@@ -115,14 +115,8 @@ int coulomb_nsplit(long tile_elems, long naux, int elems_per_thread) {
 // The capped forms ask for the largest shared-memory carveout, the one the half-transform runs with, so that
 // their CTAs can share its SMs.  The forms run alone keep the default (their L1 caches w and Dt).
 static void prefer_shared_carveout() {
-  static const bool once = [] {
-    cudaFuncSetAttribute(k_coulomb_w<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    cudaFuncSetAttribute(k_coulomb_j<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    return true;
-  }();
-  (void)once;
+  prefer_max_shared(reinterpret_cast<const void*>(k_coulomb_w<true>));
+  prefer_max_shared(reinterpret_cast<const void*>(k_coulomb_j<true>));
 }
 
 void launch_coulomb_w(const double* B, const double* Dt, long naux, long tile_elems, double* w, cudaStream_t s,

@@ -143,12 +143,7 @@ static void launch_xform_nf(const double* B, const double* MOp, long naux, long 
   constexpr int A_STAGE = (64 * XK > KC * LDM) ? 64 * XK : KC * LDM;
   size_t smem = (2 * A_STAGE + 2 * NOCCP * XK) * sizeof(double);
   ensure_smem_limit(reinterpret_cast<const void*>(k_xform_f64<NF>), smem);
-  static const bool carveout = [] {  // room for three CTAs an SM
-    cudaFuncSetAttribute(k_xform_f64<NF>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    return true;
-  }();
-  (void)carveout;
+  prefer_max_shared(reinterpret_cast<const void*>(k_xform_f64<NF>));  // room for three CTAs an SM
   long npad = nt * TILE;
   long tile_elems = nt * (nt + 1) / 2 * TILE2;
   dim3 grid(static_cast<unsigned>(nt * nb), static_cast<unsigned>(naux));

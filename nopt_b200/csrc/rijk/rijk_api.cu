@@ -77,6 +77,21 @@ cudaError_t ensure_smem_limit(const void* fn, size_t bytes) {
   return e;
 }
 
+void prefer_max_shared(const void* fn) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, bool> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  bool& set = done[{fn, dev}];
+  if (set) return;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) ==
+      cudaSuccess)
+    set = true;
+  else
+    cudaGetLastError();  // a hint only: the launch works without it
+}
+
 void release(DeviceBuf& b) {
   if (b.p) cudaFree(b.p);
   b.p = nullptr;

@@ -138,6 +138,9 @@ int check_device_error(rijk_ctx* ctx);
 // attribute lives in each device's context, so it is set once per (kernel, device), not once per
 // process: a process that drives several GPUs sets it on each.
 cudaError_t ensure_smem_limit(const void* fn, size_t bytes);
+// The largest shared-memory carveout for fn on the current device (a hint for co-resident CTAs), set
+// once per (kernel, device) as above.
+void prefer_max_shared(const void* fn);
 int check_fock_args(rijk_ctx* ctx, long nocc, int precision);
 // One JSON line per Fock build (and per rijk_scf) appended to the file named by the environment
 // variable RIJK_LOG, when it is set: the call, sizes, precision, device times, algorithmic FLOPs and
