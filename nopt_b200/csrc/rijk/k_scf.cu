@@ -356,6 +356,156 @@ __global__ void __launch_bounds__(256) k_tc2_update_sym(double* __restrict__ P, 
   }
 }
 
+// ---- one TC2 step in one kernel, for n' < 1024.  At n' = 384 a step of the form above (the library
+// product, then the trace and update kernels) took about 23 us, most of it launch latency.  Here a CTA of
+// 4 warps forms a 32 x 32 tile of P^2 on DMMA (warps 2 x 2, 16 x 16 each) over 32-wide chunks of k
+// staged [k][row] (stride T2_LD, conflict-free as in dmma.cuh).  P is symmetric, so P(k, j) = P(j, k):
+// both operands are columns of P, with the rows contiguous.  The choice between P^2 and 2P - P^2 needs
+// tr P and tr P^2 = ||P||_F^2 of the input, which the previous step (or k_tc2_norms) left as partial sums,
+// one pair per tile: lane 0 of warp 0 of every CTA adds them in the same fixed order, so every CTA, and
+// every rank of a sharded SCF, takes the same branch.  The epilogue writes Pn and its tile's own partial
+// sums; CTA (0, 0) also writes tr P and tr P^2 to sc[1], sc[2] for the host's convergence test.
+constexpr int T2 = 32;
+constexpr int T2_LD = 36;
+constexpr int T2_THREADS = 128;
+
+__device__ __forceinline__ void t2_cp8(double* smem, const double* gmem, bool valid) {
+  const uint32_t d = smem_u32(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gmem), "r"(valid ? 8 : 0));
+}
+
+// this CTA's (sum of the diagonal, sum of squares) of v over its threads, in a fixed order
+__device__ __forceinline__ void t2_tile_sums(double sdg, double ssq, double* __restrict__ part_out) {
+  __shared__ double red[2][T2_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sdg += __shfl_down_sync(0xffffffffu, sdg, o);
+    ssq += __shfl_down_sync(0xffffffffu, ssq, o);
+  }
+  if (lane == 0) {
+    red[0][warp] = sdg;
+    red[1][warp] = ssq;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const long blk = static_cast<long>(blockIdx.y) * gridDim.x + blockIdx.x;
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < T2_THREADS / 32; ++w) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    part_out[2 * blk] = a;
+    part_out[2 * blk + 1] = b;
+  }
+}
+
+// The partial sums of P0 (column-major n x n), one pair per 32 x 32 tile of the step's grid.
+__global__ void __launch_bounds__(T2_THREADS) k_tc2_norms(const double* __restrict__ P, long n,
+                                                          double* __restrict__ part_out) {
+  const long r0 = static_cast<long>(blockIdx.y) * T2, c0 = static_cast<long>(blockIdx.x) * T2;
+  double sdg = 0.0, ssq = 0.0;
+  for (int e = threadIdx.x; e < T2 * T2; e += T2_THREADS) {
+    const long r = r0 + (e & 31), c = c0 + (e >> 5);
+    if (r < n && c < n) {
+      const double v = P[r + c * n];
+      ssq += v * v;
+      if (r == c) sdg += v;
+    }
+  }
+  t2_tile_sums(sdg, ssq, part_out);
+}
+
+__global__ void __launch_bounds__(T2_THREADS) k_tc2_step(const double* __restrict__ P, double* __restrict__ Pn, long n,
+                                                         const double* __restrict__ part_in,
+                                                         double* __restrict__ part_out, double nocc,
+                                                         double* __restrict__ sc) {
+  __shared__ __align__(16) double sA[2][T2 * T2_LD];
+  __shared__ __align__(16) double sB[2][T2 * T2_LD];
+  __shared__ double tr[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long r0 = static_cast<long>(blockIdx.y) * T2, c0 = static_cast<long>(blockIdx.x) * T2;
+  const int nblk = gridDim.x * gridDim.y;
+  if (warp == 0) {  // tr P and ||P||_F^2 from the input's partial sums, in a fixed order
+    double a = 0.0, b = 0.0;
+    for (int i = lane; i < nblk; i += 32) {
+      a += part_in[2 * i];
+      b += part_in[2 * i + 1];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      tr[0] = a;
+      tr[1] = b;
+      if (blockIdx.x == 0 && blockIdx.y == 0) {
+        sc[1] = a;
+        sc[2] = b;
+      }
+    }
+  }
+  auto load = [&](int st, long k0) {  // element (row, k) of a column block: P[row + k n]
+    for (int e = tid; e < T2 * T2; e += T2_THREADS) {
+      const int kk = e >> 5, rr = e & 31;
+      const long k = k0 + kk, ra = r0 + rr, rb = c0 + rr;
+      const bool va = k < n && ra < n, vb = k < n && rb < n;
+      t2_cp8(&sA[st][kk * T2_LD + rr], va ? P + ra + k * n : P, va);
+      t2_cp8(&sB[st][kk * T2_LD + rr], vb ? P + rb + k * n : P, vb);
+    }
+  };
+  const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
+  double acc[2][2][2] = {};
+  const long nk = (n + T2 - 1) / T2;
+  load(0, 0);
+  cp_async_commit();
+  for (long kc = 0; kc < nk; ++kc) {
+    if (kc + 1 < nk) {
+      load(static_cast<int>((kc + 1) & 1), (kc + 1) * T2);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double* a_ = sA[kc & 1];
+    const double* b_ = sB[kc & 1];
+#pragma unroll
+    for (int k = 0; k < T2; k += 4) {
+      double a[2], b[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) a[i] = a_[(k + t) * T2_LD + wm * 16 + i * 8 + g];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) b[j] = b_[(k + t) * T2_LD + wn * 16 + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+  const double t1 = tr[0], t2 = tr[1];
+  const bool square = fabs(t2 - nocc) < fabs(2.0 * t1 - t2 - nocc);
+  double sdg = 0.0, ssq = 0.0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long r = r0 + wm * 16 + i * 8 + g, c = c0 + wn * 16 + j * 8 + 2 * t + h;
+        if (r < n && c < n) {
+          const double s2 = acc[i][j][h];
+          const double v = square ? s2 : 2.0 * P[r + c * n] - s2;
+          Pn[r + c * n] = v;
+          ssq += v * v;
+          if (r == c) sdg += v;
+        }
+      }
+  t2_tile_sums(sdg, ssq, part_out);
+}
+
 // One block: sc[slot] = min_i |R_ii| / max_i |R_ii| of a Cholesky factor (n x n, column-major)
 __global__ void k_chol_ratio(const double* __restrict__ R, long n, double* __restrict__ sc, int slot) {
   __shared__ double sh[2][32];
@@ -476,8 +626,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
             &dC = wb[7], &dJK = wb[8], &dT1 = wb[10], &dT2 = wb[11], &dE = wb[12], &dW = wb[13],
             &dU = wb[14], &work = wb[15], &info = wb[16], &red = wb[17], &out = wb[18], &ring_F = wb[19],
             &ring_E = wb[20];
-  // occupied eigenvectors (X basis), purification scalars, Cholesky infos
-  DeviceBuf &dV = wb[21], &dPur = wb[22], &dInfo2 = wb[23];
+  // occupied eigenvectors (X basis), purification scalars, Cholesky infos, the fused TC2 steps' partial sums
+  DeviceBuf &dV = wb[21], &dPur = wb[22], &dInfo2 = wb[23], &dPart = wb[28];
   auto cleanup = [&]() {};  // nothing to free: the buffers stay with the context
   const size_t b_nn = nn * sizeof(double);
   if ((rc = ensure(ctx, dH, b_nn, "scf H")) || (rc = ensure(ctx, dS, b_nn, "scf S")) ||
@@ -494,6 +644,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
       (rc = ensure(ctx, ring_E, static_cast<size_t>(m_max) * b_nn, "scf DIIS e")) ||
       (rc = ensure(ctx, dV, static_cast<size_t>(n) * std::max<long>(nocc, 1) * sizeof(double), "scf V")) ||
       (rc = ensure(ctx, dPur, 16 * sizeof(double), "scf purification")) ||
+      (rc = ensure(ctx, dPart, 4 * 32 * 32 * sizeof(double), "scf purification partial sums")) ||
       (rc = ensure(ctx, dInfo2, 4 * sizeof(int), "scf Cholesky info"))) {
     cleanup();
     return rc;
@@ -662,15 +813,25 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     k_purify_init<<<grid_of(nm * nm), 256, 0, s>>>(P, nm, pPur);
     int left = -1;  // steps still to take once the idempotency error is small
     bool done = false;
+    // below n' = 1024 each step is one fused kernel, alternating between P and P2 (k_tc2_step)
+    const bool fused = nm < 1024;
+    const unsigned nb2 = static_cast<unsigned>((nm + T2 - 1) / T2);
+    double* part = static_cast<double*>(dPart.p);
+    const long pstride = 2L * nb2 * nb2;
+    double* Pa = P;   // the current iterate of the fused steps
+    double* Pb = P2;
+    if (fused) k_tc2_norms<<<dim3(nb2, nb2), T2_THREADS, 0, s>>>(P, nm, part);
     for (int step = 1; step <= kMaxSteps && !done; ++step) {
-      // P^2: its upper triangle is read.  DSYRK forms half the products; below n' = 1024 cuBLAS's
-      // DGEMM was the faster of the two (21 against 25 ms of steps per SCF at n' = 384)
-      if (nm >= 1024)
+      if (fused) {
+        k_tc2_step<<<dim3(nb2, nb2), T2_THREADS, 0, s>>>(Pa, Pb, nm, part + ((step - 1) & 1) * pstride,
+                                                         part + (step & 1) * pstride, static_cast<double>(nocc), pPur);
+        std::swap(Pa, Pb);
+      } else {
+        // P^2: its upper triangle is read (DSYRK forms half the products)
         cublasDsyrk(cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nmi, nmi, &one, P, nmi, &zero, P2, nmi);
-      else
-        cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, nmi, nmi, nmi, &one, P, nmi, P, nmi, &zero, P2, nmi);
-      k_tc2_traces<<<1, 256, 0, s>>>(P, P2, nm, pPur);
-      k_tc2_update_sym<<<static_cast<unsigned>(ntiles32), 256, 0, s>>>(P, P2, nm, pPur, static_cast<double>(nocc));
+        k_tc2_traces<<<1, 256, 0, s>>>(P, P2, nm, pPur);
+        k_tc2_update_sym<<<static_cast<unsigned>(ntiles32), 256, 0, s>>>(P, P2, nm, pPur, static_cast<double>(nocc));
+      }
       if (left > 0) {
         done = --left == 0;
       } else if (step >= 16 && step % 4 == 0) {
@@ -681,6 +842,7 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
         if (std::fabs(sc[1] - sc[2]) < 1e-8) left = 2;  // quadratic from here: two steps reach rounding
       }
     }
+    if (fused && Pa != P) cudaMemcpyAsync(P, Pa, static_cast<size_t>(nm) * nm * sizeof(double), cudaMemcpyDeviceToDevice, s);
     if (!done) return 1;
     // W = P V, orthonormalised: W^T W = U^T U, W <- W U^-1, twice
     cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, nmi, no, nmi, &one, P, nmi, pV, nmi, &zero, pT1, nmi);
