@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(256) k_tc2_update_sym(double* __restrict__ P, 
   }
 }
 
-// ---- one TC2 step in one kernel, for n' < 1024.  At n' = 384 a step of the form above (the library
+// ---- one TC2 step in one kernel, for n' <= 512.  At n' = 384 a step of the form above (the library
 // product, then the trace and update kernels) took about 23 us, most of it launch latency.  Here a CTA of
 // 4 warps forms a 32 x 32 tile of P^2 on DMMA (warps 2 x 2, 16 x 16 each) over 32-wide chunks of k
 // staged [k][row] (stride T2_LD, conflict-free as in dmma.cuh).  P is symmetric, so P(k, j) = P(j, k):
@@ -813,8 +813,10 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     k_purify_init<<<grid_of(nm * nm), 256, 0, s>>>(P, nm, pPur);
     int left = -1;  // steps still to take once the idempotency error is small
     bool done = false;
-    // below n' = 1024 each step is one fused kernel, alternating between P and P2 (k_tc2_step)
-    const bool fused = nm < 1024;
+    // up to n' = 512 each step is one fused kernel, alternating between P and P2 (k_tc2_step).  Measured: the
+    // fused steps won at n' = 144 and 384 (the SCF 24.5 -> 19.9 ms and 77 -> 72 ms), the library's DGEMM at
+    // n' = 970 (1280 against 1289 ms), where the product, not the launches, sets a step's time.
+    const bool fused = nm <= 512;
     const unsigned nb2 = static_cast<unsigned>((nm + T2 - 1) / T2);
     double* part = static_cast<double*>(dPart.p);
     const long pstride = 2L * nb2 * nb2;
@@ -827,8 +829,12 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
                                                          part + (step & 1) * pstride, static_cast<double>(nocc), pPur);
         std::swap(Pa, Pb);
       } else {
-        // P^2: its upper triangle is read (DSYRK forms half the products)
-        cublasDsyrk(cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nmi, nmi, &one, P, nmi, &zero, P2, nmi);
+        // P^2: its upper triangle is read.  DSYRK forms half the products; below n' = 1024 cuBLAS's DGEMM
+        // was the faster of the two (21 against 25 ms of steps per SCF at n' = 384)
+        if (nm >= 1024)
+          cublasDsyrk(cb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nmi, nmi, &one, P, nmi, &zero, P2, nmi);
+        else
+          cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, nmi, nmi, nmi, &one, P, nmi, P, nmi, &zero, P2, nmi);
         k_tc2_traces<<<1, 256, 0, s>>>(P, P2, nm, pPur);
         k_tc2_update_sym<<<static_cast<unsigned>(ntiles32), 256, 0, s>>>(P, P2, nm, pPur, static_cast<double>(nocc));
       }
