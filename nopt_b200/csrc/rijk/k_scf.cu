@@ -416,12 +416,22 @@ __global__ void __launch_bounds__(T2_THREADS) k_tc2_norms(const double* __restri
   t2_tile_sums(sdg, ssq, part_out);
 }
 
+constexpr int T2_STAGES = 3;
+constexpr size_t T2_SMEM = static_cast<size_t>(T2_STAGES) * 2 * T2 * T2_LD * sizeof(double);
+
+// 16-byte copy of which the first `bytes` (0, 8 or 16) come from global memory, the rest zero
+__device__ __forceinline__ void t2_cp16(double* smem, const double* gmem, int bytes) {
+  const uint32_t d = smem_u32(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gmem), "r"(bytes));
+}
+
+// PAIRS: n is even, so (row, k) pairs of rows start on 16-byte boundaries and move as one copy
+template <bool PAIRS>
 __global__ void __launch_bounds__(T2_THREADS) k_tc2_step(const double* __restrict__ P, double* __restrict__ Pn, long n,
                                                          const double* __restrict__ part_in,
                                                          double* __restrict__ part_out, double nocc,
                                                          double* __restrict__ sc) {
-  __shared__ __align__(16) double sA[2][T2 * T2_LD];
-  __shared__ __align__(16) double sB[2][T2 * T2_LD];
+  extern __shared__ __align__(16) double t2s[];  // T2_STAGES x {A, B} chunks of [k][row]
   __shared__ double tr[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long r0 = static_cast<long>(blockIdx.y) * T2, c0 = static_cast<long>(blockIdx.x) * T2;
@@ -446,13 +456,27 @@ __global__ void __launch_bounds__(T2_THREADS) k_tc2_step(const double* __restric
       }
     }
   }
+  auto stage_a = [&](int st) { return t2s + static_cast<size_t>(st) * 2 * T2 * T2_LD; };
   auto load = [&](int st, long k0) {  // element (row, k) of a column block: P[row + k n]
-    for (int e = tid; e < T2 * T2; e += T2_THREADS) {
-      const int kk = e >> 5, rr = e & 31;
-      const long k = k0 + kk, ra = r0 + rr, rb = c0 + rr;
-      const bool va = k < n && ra < n, vb = k < n && rb < n;
-      t2_cp8(&sA[st][kk * T2_LD + rr], va ? P + ra + k * n : P, va);
-      t2_cp8(&sB[st][kk * T2_LD + rr], vb ? P + rb + k * n : P, vb);
+    double* sA = stage_a(st);
+    double* sB = sA + T2 * T2_LD;
+    if (PAIRS) {
+      for (int e = tid; e < T2 * T2 / 2; e += T2_THREADS) {
+        const int kk = e >> 4, rr = (e & 15) * 2;
+        const long k = k0 + kk, ra = r0 + rr, rb = c0 + rr;
+        const int ba = k < n ? static_cast<int>(8 * std::max<long>(0, std::min<long>(2, n - ra))) : 0;
+        const int bb = k < n ? static_cast<int>(8 * std::max<long>(0, std::min<long>(2, n - rb))) : 0;
+        t2_cp16(&sA[kk * T2_LD + rr], ba ? P + ra + k * n : P, ba);
+        t2_cp16(&sB[kk * T2_LD + rr], bb ? P + rb + k * n : P, bb);
+      }
+    } else {
+      for (int e = tid; e < T2 * T2; e += T2_THREADS) {
+        const int kk = e >> 5, rr = e & 31;
+        const long k = k0 + kk, ra = r0 + rr, rb = c0 + rr;
+        const bool va = k < n && ra < n, vb = k < n && rb < n;
+        t2_cp8(&sA[kk * T2_LD + rr], va ? P + ra + k * n : P, va);
+        t2_cp8(&sB[kk * T2_LD + rr], vb ? P + rb + k * n : P, vb);
+      }
     }
   };
   const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
@@ -460,17 +484,23 @@ __global__ void __launch_bounds__(T2_THREADS) k_tc2_step(const double* __restric
   const long nk = (n + T2 - 1) / T2;
   load(0, 0);
   cp_async_commit();
+  if (nk > 1) {
+    load(1, T2);
+    cp_async_commit();
+  }
   for (long kc = 0; kc < nk; ++kc) {
-    if (kc + 1 < nk) {
-      load(static_cast<int>((kc + 1) & 1), (kc + 1) * T2);
+    if (kc + 2 < nk) {
+      load(static_cast<int>((kc + 2) % T2_STAGES), (kc + 2) * T2);
       cp_async_commit();
+      cp_async_wait<2>();
+    } else if (kc + 1 < nk) {
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    const double* a_ = sA[kc & 1];
-    const double* b_ = sB[kc & 1];
+    const double* a_ = stage_a(static_cast<int>(kc % T2_STAGES));
+    const double* b_ = a_ + T2 * T2_LD;
 #pragma unroll
     for (int k = 0; k < T2; k += 4) {
       double a[2], b[2];
@@ -504,6 +534,19 @@ __global__ void __launch_bounds__(T2_THREADS) k_tc2_step(const double* __restric
         }
       }
   t2_tile_sums(sdg, ssq, part_out);
+}
+
+// One fused step; the launch configuration for n' (even n': 16-byte copies).
+void launch_tc2_step(const double* P, double* Pn, long n, const double* part_in, double* part_out, double nocc,
+                     double* sc, cudaStream_t s) {
+  const unsigned nb = static_cast<unsigned>((n + T2 - 1) / T2);
+  if (n % 2 == 0) {
+    ensure_smem_limit(reinterpret_cast<const void*>(k_tc2_step<true>), T2_SMEM);
+    k_tc2_step<true><<<dim3(nb, nb), T2_THREADS, T2_SMEM, s>>>(P, Pn, n, part_in, part_out, nocc, sc);
+  } else {
+    ensure_smem_limit(reinterpret_cast<const void*>(k_tc2_step<false>), T2_SMEM);
+    k_tc2_step<false><<<dim3(nb, nb), T2_THREADS, T2_SMEM, s>>>(P, Pn, n, part_in, part_out, nocc, sc);
+  }
 }
 
 // One block: sc[slot] = min_i |R_ii| / max_i |R_ii| of a Cholesky factor (n x n, column-major)
@@ -825,8 +868,8 @@ RIJK_API int rijk_scf(rijk_ctx* ctx, const double* H, const double* S, long nocc
     if (fused) k_tc2_norms<<<dim3(nb2, nb2), T2_THREADS, 0, s>>>(P, nm, part);
     for (int step = 1; step <= kMaxSteps && !done; ++step) {
       if (fused) {
-        k_tc2_step<<<dim3(nb2, nb2), T2_THREADS, 0, s>>>(Pa, Pb, nm, part + ((step - 1) & 1) * pstride,
-                                                         part + (step & 1) * pstride, static_cast<double>(nocc), pPur);
+        launch_tc2_step(Pa, Pb, nm, part + ((step - 1) & 1) * pstride, part + (step & 1) * pstride,
+                        static_cast<double>(nocc), pPur, s);
         std::swap(Pa, Pb);
       } else {
         // P^2: its upper triangle is read.  DSYRK forms half the products; below n' = 1024 cuBLAS's DGEMM
