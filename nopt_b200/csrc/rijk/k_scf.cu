@@ -359,7 +359,8 @@ __global__ void __launch_bounds__(256) k_tc2_update_sym(double* __restrict__ P, 
 // ---- one TC2 step in one kernel, for n' <= 512.  At n' = 384 a step of the form above (the library
 // product, then the trace and update kernels) took about 23 us, most of it launch latency.  Here a CTA of
 // 4 warps forms a 32 x 32 tile of P^2 on DMMA (warps 2 x 2, 16 x 16 each) over 32-wide chunks of k
-// staged [k][row] (stride T2_LD, conflict-free as in dmma.cuh).  P is symmetric, so P(k, j) = P(j, k):
+// staged [k][row] (stride T2_LD, conflict-free as in dmma.cuh) through a three-stage cp.async pipeline.
+// P is symmetric, so P(k, j) = P(j, k):
 // both operands are columns of P, with the rows contiguous.  The choice between P^2 and 2P - P^2 needs
 // tr P and tr P^2 = ||P||_F^2 of the input, which the previous step (or k_tc2_norms) left as partial sums,
 // one pair per tile: lane 0 of warp 0 of every CTA adds them in the same fixed order, so every CTA, and
